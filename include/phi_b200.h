@@ -1,0 +1,177 @@
+/*
+ * phi_b200.h -- C ABI of the B200-native HEOM integrator.
+ *
+ * This library is a drop-in for the time-propagation (RK4, RKF45) and
+ * steady-state (BiCGSTAB) paths of the PHI parallel hierarchy integrator.
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (PHI_OK = 0); the C++ facade in include/phi/ (PhiParameters,
+ * HierarchyIntegrator) is written on top of it.  Each declaration names the
+ * reference interface it replaces (paths relative to the PHI source tree).
+ *
+ * Conventions shared with PHI:
+ *  - complex numbers are interleaved (re, im) doubles;
+ *  - every N x N matrix (Hamiltonian, rho(0), rho_0, each auxiliary density
+ *    operator) is column-major: element (r, c) at index r + c*N
+ *    (parameter_input.cc:244-339 fills H[r + c*N] from file row r);
+ *  - the full hierarchy state is node-major in PHI's node-id order
+ *    (hierarchy.cc:45-155): node i occupies elements [i*N*N, (i+1)*N*N).
+ *  - units are the caller's: PHI's defaults are hbar = 5.3088354 cm^-1 ps,
+ *    k_B = 0.6950344 cm^-1/K (phi_parameters.h:13-16).
+ *
+ * Threading: a context is single-owner; calls on one context must not
+ * overlap.  Distinct contexts are independent.
+ */
+#ifndef PHI_B200_H_
+#define PHI_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define PHI_OK 0
+#define PHI_E_INVALID 1        /* invalid or unsupported parameters */
+#define PHI_E_OOM 2            /* device or host allocation failed */
+#define PHI_E_BUDGET 3         /* hierarchy larger than the node budget */
+#define PHI_E_STEP_COLLAPSE 4  /* RKF45 step limit reached */
+#define PHI_E_NO_CONVERGENCE 5 /* iterative solve hit its iteration limit */
+#define PHI_E_TIMEOUT 6        /* a bounded device wait gave up */
+#define PHI_E_CUDA 7           /* CUDA runtime error */
+#define PHI_E_STATE 8          /* call made in the wrong state */
+#define PHI_E_NUMERIC 9        /* non-finite values appeared */
+
+/* Bath models: HierarchyUpdater subclasses (hierarchy_updater.h:24-436). */
+#define PHI_BATH_INDEPENDENT 0 /* IndependentBath: bath j couples to |s_j><s_j| */
+#define PHI_BATH_DIAGONAL 1    /* DiagonalBath: CorrelatedCouplingTerms */
+#define PHI_BATH_FULL 2        /* FullBath: FullBathTerms */
+
+/* Arithmetic of the Liouvillian applies. */
+#define PHI_PREC_FP64 0  /* complex128 everywhere */
+#define PHI_PREC_MIXED 1 /* FP32 stage arithmetic, FP64 state / norms / control */
+
+/* Problem description: the PhiParameters fields the path reads
+ * (phi_parameters.h:32-122).  Arrays are borrowed for the duration of the
+ * create call only. */
+typedef struct {
+  int32_t num_states;          /* num_states (N) */
+  int32_t num_baths;           /* num_bath_couplings */
+  int32_t num_matsubara_terms; /* num_matsubara_terms: K + 1, as PHI stores it */
+  int32_t truncation_level;    /* hierarchy_truncation_level: tiers incl. tier 0 */
+  int32_t bath_kind;           /* PHI_BATH_* */
+  int32_t normalized;          /* is_rho_normalized */
+  double hbar;                 /* hbar */
+  double boltzmann_constant;   /* boltzmann_constant */
+  double temperature;          /* temperature */
+  const double *hamiltonian;   /* time_indepenent_hamiltonian: 2*N*N */
+  const double *gamma;         /* gamma: num_baths */
+  const double *lambda;        /* lambda: num_baths */
+  const double *coupling;      /* bath_coupling_op: diagonal num_baths*N,
+                                  full num_baths*N*N (real); NULL otherwise */
+  const int32_t *bath_sites;   /* independent baths: site of each bath, NULL
+                                  for PHI's identity map (bath j on |j><j|) */
+  const double *initial_density_matrix; /* initial_density_matrix: 2*N*N */
+  int32_t precision;           /* PHI_PREC_* */
+  int32_t device;              /* CUDA device ordinal */
+  int64_t max_nodes;           /* node budget; 0 = limited by memory only */
+} phi_problem_desc;
+
+typedef struct phi_ctx phi_ctx;
+
+/* RKF45 run statistics (Rkf45Integrate's "#Total number of integration
+ * steps" / "accepted integration steps", hierarchy_integrator.cc:2545-2550). */
+typedef struct {
+  int64_t steps;       /* attempted steps */
+  int64_t accepted;    /* accepted steps */
+  double final_time;   /* time reached */
+  double final_dt;     /* step size after the last step */
+  double max_error;    /* largest accepted step error estimate */
+} phi_rkf45_stats;
+
+/* Steady-state solve statistics. */
+typedef struct {
+  int32_t iterations;    /* BiCGSTAB iterations */
+  int32_t converged;     /* 1 if the residual tolerance was met */
+  double residual;       /* final ||r||_2 / ||b||_2 */
+  double seconds;        /* device time of the solve */
+} phi_solve_stats;
+
+/* Builds the hierarchy on the device, uploads constants and sets the initial
+ * state.  Replaces HierarchyIntegrator(PhiParameters*) plus the setup half of
+ * Launch(): Initialize, ConstructI, LinkHierarchyNodes, InitializePrefactors,
+ * InitializeDensityMatrix (hierarchy_integrator.cc:49-62, :376-594,
+ * :1038-1158, :1204-1466; hierarchy.cc:45-155). */
+int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out);
+
+/* Same, from a PHI parameter file (PhiParameters::ReadInputFile and
+ * FixIncompatibleCombinations, phi_parameters.cc:152-888).  method is one of
+ * "rk4", "rkf45", "bicgstab" (decides the forced normalisation exactly as
+ * FixIncompatibleCombinations does). */
+int phi_gpu_create_from_file(const char *path, const char *method, int32_t precision,
+                             int32_t device, phi_ctx **out);
+
+/* Releases every device and host resource of the context. */
+int phi_gpu_destroy(phi_ctx *ctx);
+
+/* Hierarchy size: M nodes, T = num_baths * (K+1) terms, N states. */
+int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
+                 int32_t *num_states);
+
+/* Node table built on the device, copied to host buffers of M*T int32 each
+ * (any may be NULL): multi_index[i*T + t] = n_t of node i; next[i*T + t] =
+ * id of node i + e_t or -1; prev[i*T + t] = id of node i - e_t or -1.
+ * Replaces the multi_index_map_ of ConstructI (hierarchy.cc:45-155) and the
+ * neighbour lists of LinkHierarchyNodes (hierarchy_integrator.cc:1204-1338). */
+int phi_gpu_get_node_table(const phi_ctx *ctx, int32_t *multi_index, int32_t *next,
+                           int32_t *prev);
+
+/* Whole-hierarchy state, host buffers of 2*M*N*N doubles. */
+int phi_gpu_set_state(phi_ctx *ctx, const double *state);
+int phi_gpu_get_state(const phi_ctx *ctx, double *state);
+
+/* rho_0 (node 0), host buffer of 2*N*N doubles.  Replaces density_matrix()
+ * (hierarchy_integrator.cc:177-191), which returns the same storage order. */
+int phi_gpu_get_rho0(const phi_ctx *ctx, double *rho0);
+
+/* One Liouvillian apply over every node: out = L(in), host buffers of
+ * 2*M*N*N doubles.  Replaces a sweep of HierarchyUpdater::Get
+ * (hierarchy_updater.h:36-52) over all nodes.  Input ADOs must be Hermitian
+ * (PHI's formulation keeps every ADO Hermitian). */
+int phi_gpu_apply(phi_ctx *ctx, const double *in, double *out);
+
+/* Device-pointer variant: in/out are device buffers of M*N*N complex in the
+ * context's precision; stream is a cudaStream_t (NULL = legacy default). */
+int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream);
+
+/* Fixed-step RK4 from the current state (Rk4Integrate,
+ * hierarchy_integrator.cc:2578-2939).  Steps while time < t_end with time
+ * advanced by repeated addition of dt, as the reference does.  After step i
+ * (0-based) with i % ceil(output_min_step/dt) == 0, rho_0 is written to
+ * traj[k*2*N*N] and its time to times[k] for k < capacity (either may be
+ * NULL).  Returns the number of steps and of output rows. */
+int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min_step,
+                double *traj, double *times, int64_t capacity, int64_t *num_steps,
+                int64_t *num_out);
+
+/* Adaptive RKF45 from the current state (Rkf45Integrate,
+ * hierarchy_integrator.cc:1797-2573): max-abs error over every ADO element,
+ * accept if error < tol or dt/2 < min_dt, grow x1.1 when error < tol/10,
+ * shrink x0.5 on reject, last step clamped to t_end.  max_steps bounds the
+ * attempted steps (0 = 10^7); hitting it returns PHI_E_STEP_COLLAPSE. */
+int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
+                  int64_t max_steps, phi_rkf45_stats *stats);
+
+/* Time carried by the context (advanced by the integrators). */
+int phi_gpu_get_time(const phi_ctx *ctx, double *time);
+int phi_gpu_set_time(phi_ctx *ctx, double time);
+
+/* Copies the text of the last error on this context (or of the last failed
+ * create when ctx is NULL) into buf. */
+int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PHI_B200_H_ */

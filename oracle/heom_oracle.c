@@ -1,0 +1,633 @@
+/*
+ * heom_oracle.c -- CPU restatement of the PHI HEOM path.  TEST
+ * INFRASTRUCTURE ONLY (see heom_oracle.h): the checker for the CUDA kernels,
+ * never part of the product library.
+ *
+ * The arithmetic follows the reference's -DNOBLAS code path operation by
+ * operation (its Gemm loop, blas_wrapper.cc:11-34, stands in for every
+ * zhemm), so results agree with the reference build to rounding.  Citations
+ * are relative to the PHI source tree (src/...).
+ */
+#include "heom_oracle.h"
+
+#include <complex.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef double complex cplx;
+
+/* hierarchy_node.h:7 */
+static const double kPi = 3.14159265358979323846264338327950288419716939937510;
+
+struct oracle_ctx {
+  int N, nb, K1, T, trunc, kind, normalized;
+  double hbar, kb, temp;
+  int64_t M;
+  int32_t *mi;     /* M*T multi-indices */
+  int32_t *next;   /* M*T: id of n + e_t, -1 when absent */
+  int32_t *prev;   /* M*T: id of n - e_t, -1 when absent */
+  int32_t *tier;   /* M: sum of the multi-index */
+  cplx *H, *Hadj;  /* N*N */
+  cplx *corr;      /* T: correlation-function constants c_t */
+  double *abs_corr;
+  cplx *matsubara; /* nb: Matsubara/residual correction Delta_j */
+  double *gamma;   /* nb */
+  cplx *bath;      /* diagonal: nb*N; full: nb*N*N */
+  cplx *same, *nextop, *prevop; /* diagonal / full bath operator tables */
+};
+
+/* ------------------------------------------------------------------------ */
+/* Multi-index hash set (stands in for the std::map of hierarchy.h:34-35).   */
+
+typedef struct {
+  int64_t *slot; /* node id or -1 */
+  int64_t mask;
+  const int32_t *keys; /* node-major multi-indices */
+  int T;
+} index_set;
+
+static uint64_t hash_index(const int32_t *v, int T) {
+  uint64_t h = 1469598103934665603ULL;
+  for (int i = 0; i < T; ++i) {
+    h ^= (uint64_t)(uint32_t)v[i] + 0x9e3779b97f4a7c15ULL;
+    h *= 1099511628211ULL;
+    h ^= h >> 29;
+  }
+  return h;
+}
+
+static int set_init(index_set *s, int64_t capacity, const int32_t *keys, int T) {
+  int64_t size = 16;
+  while (size < 2 * capacity + 16) size <<= 1;
+  s->slot = (int64_t *)malloc(sizeof(int64_t) * size);
+  if (!s->slot) return -1;
+  for (int64_t i = 0; i < size; ++i) s->slot[i] = -1;
+  s->mask = size - 1;
+  s->keys = keys;
+  s->T = T;
+  return 0;
+}
+
+/* Returns the id stored for v, or -1. */
+static int64_t set_find(const index_set *s, const int32_t *v) {
+  int64_t h = (int64_t)(hash_index(v, s->T) & (uint64_t)s->mask);
+  for (;;) {
+    int64_t id = s->slot[h];
+    if (id < 0) return -1;
+    if (memcmp(s->keys + id * s->T, v, sizeof(int32_t) * s->T) == 0) return id;
+    h = (h + 1) & s->mask;
+  }
+}
+
+static void set_insert(index_set *s, int64_t id) {
+  const int32_t *v = s->keys + id * s->T;
+  int64_t h = (int64_t)(hash_index(v, s->T) & (uint64_t)s->mask);
+  while (s->slot[h] >= 0) h = (h + 1) & s->mask;
+  s->slot[h] = id;
+}
+
+/* ------------------------------------------------------------------------ */
+
+int64_t oracle_node_count(int num_terms, int truncation) {
+  /* C(T + L, L) with L = truncation - 1 (phi_parameters.cc:1138-1147). */
+  if (num_terms < 0 || truncation < 1) return -1;
+  int64_t L = truncation - 1;
+  long double acc = 1.0L;
+  int64_t c = 1;
+  for (int64_t i = 1; i <= L; ++i) {
+    acc = acc * (num_terms + i) / i;
+    if (acc > 9.0e18L) return -1;
+    c = (int64_t)(acc + 0.5L);
+  }
+  return c;
+}
+
+int64_t oracle_build_hierarchy(int T, int truncation, int32_t *mi, int64_t capacity) {
+  /* Hierarchy::ConstructI, hierarchy.cc:45-155. */
+  int64_t M = oracle_node_count(T, truncation);
+  if (M < 0 || M > capacity) return -1;
+  index_set set;
+  if (set_init(&set, M, mi, T) != 0) return -1;
+  memset(mi, 0, sizeof(int32_t) * (size_t)T);  /* tier 0: id 0 (:66-70) */
+  set_insert(&set, 0);
+  int64_t count = 1;
+  int64_t level_size = 1;
+  if (truncation >= 2) {
+    /* tier 1: id t+1 = e_t (:77-96). */
+    for (int t = 0; t < T; ++t) {
+      int32_t *v = mi + (int64_t)(t + 1) * T;
+      memset(v, 0, sizeof(int32_t) * (size_t)T);
+      v[t] = 1;
+      set_insert(&set, t + 1);
+    }
+    count += T;
+    level_size = T;
+  }
+  int32_t *cand = (int32_t *)malloc(sizeof(int32_t) * (size_t)(T + 1));
+  for (int level = 2; level < truncation; ++level) {
+    /* (:99-143) for each position k, for each node n of the previous tier,
+     * candidate = node + e_{(n+k) mod T}; appended when not yet present. */
+    const int64_t prev_first = count - level_size;
+    int64_t added = 0;
+    for (int k = 0; k < T; ++k) {
+      for (int64_t n = 0; n < level_size; ++n) {
+        memcpy(cand, mi + (prev_first + n) * T, sizeof(int32_t) * (size_t)T);
+        cand[(n + k) % T] += 1;
+        if (set_find(&set, cand) < 0) {
+          if (count + added >= M) { free(cand); free(set.slot); return -1; }
+          memcpy(mi + (count + added) * T, cand, sizeof(int32_t) * (size_t)T);
+          set_insert(&set, count + added);
+          ++added;
+        }
+      }
+    }
+    count += added;
+    level_size = added;
+  }
+  free(cand);
+  free(set.slot);
+  return count == M ? M : -1;
+}
+
+/* ------------------------------------------------------------------------ */
+
+static cplx cx(double re, double im) { return CMPLX(re, im); }
+
+oracle_ctx *oracle_create(const oracle_problem *p) {
+  oracle_ctx *c = (oracle_ctx *)calloc(1, sizeof(oracle_ctx));
+  if (!c) return NULL;
+  const int N = p->num_states;
+  c->N = N;
+  c->nb = p->num_baths;
+  c->K1 = p->num_matsubara;
+  c->T = p->num_baths * p->num_matsubara;
+  c->trunc = p->truncation;
+  c->kind = p->bath_kind;
+  c->normalized = p->normalized;
+  c->hbar = p->hbar;
+  c->kb = p->kb;
+  c->temp = p->temperature;
+  const int T = c->T;
+  c->M = oracle_node_count(T, c->trunc);
+  if (c->M <= 0) { free(c); return NULL; }
+  c->mi = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
+  c->next = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
+  c->prev = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
+  c->tier = (int32_t *)malloc(sizeof(int32_t) * (size_t)c->M);
+  if (oracle_build_hierarchy(T, c->trunc, c->mi, c->M) != c->M) {
+    oracle_destroy(c);
+    return NULL;
+  }
+  /* LinkHierarchyNodes (hierarchy_integrator.cc:1255-1330): prev for every t
+   * with n_t > 0; next for every t while tier < truncation - 1. */
+  index_set set;
+  set_init(&set, c->M, c->mi, T);
+  for (int64_t i = 0; i < c->M; ++i) set_insert(&set, i);
+  int32_t *tmp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(T + 1));
+  for (int64_t i = 0; i < c->M; ++i) {
+    const int32_t *v = c->mi + i * T;
+    int tier = 0;
+    for (int t = 0; t < T; ++t) tier += v[t];
+    c->tier[i] = tier;
+    for (int t = 0; t < T; ++t) {
+      c->prev[i * T + t] = -1;
+      c->next[i * T + t] = -1;
+      if (v[t] > 0) {
+        memcpy(tmp, v, sizeof(int32_t) * (size_t)T);
+        tmp[t] -= 1;
+        c->prev[i * T + t] = (int32_t)set_find(&set, tmp);
+      }
+      if (tier < c->trunc - 1) {
+        memcpy(tmp, v, sizeof(int32_t) * (size_t)T);
+        tmp[t] += 1;
+        c->next[i * T + t] = (int32_t)set_find(&set, tmp);
+      }
+    }
+  }
+  free(tmp);
+  free(set.slot);
+
+  c->H = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
+  c->Hadj = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
+  for (int k = 0; k < N * N; ++k) c->H[k] = cx(p->hamiltonian[2 * k], p->hamiltonian[2 * k + 1]);
+  for (int r = 0; r < N; ++r)  /* ConjugateTranspose (complex_matrix.cc) */
+    for (int col = 0; col < N; ++col) c->Hadj[r + col * N] = conj(c->H[col + r * N]);
+
+  /* Correlation-function constants, hierarchy_integrator.cc:427-473. */
+  const double hbar = p->hbar;
+  const double thermal = p->kb * p->temperature;
+  const double nu = 2 * kPi * thermal / hbar;
+  c->gamma = (double *)malloc(sizeof(double) * (size_t)(c->nb + 1));
+  for (int b = 0; b < c->nb; ++b) c->gamma[b] = p->gamma[b];
+  c->corr = (cplx *)calloc((size_t)T + 1, sizeof(cplx));
+  c->abs_corr = (double *)calloc((size_t)T + 1, sizeof(double));
+  for (int b = 0; b < c->nb; ++b) {
+    const double g = p->gamma[b], l = p->lambda[b];
+    if (g > 0) {
+      const double a = g * l / hbar;
+      const double ct = 1 / tan(g * hbar / (2 * thermal));
+      c->corr[b * c->K1] = cx(a * ct, -a);
+    }
+    c->abs_corr[b * c->K1] = cabs(c->corr[b * c->K1]);
+    for (int k = 1; k < c->K1; ++k) {
+      if (g > 0) {
+        c->corr[b * c->K1 + k] = cx(4 * l * g * thermal / hbar / hbar * (nu * k) /
+                                        (pow(nu * k, 2) - pow(g, 2)), 0.0);
+      }
+      c->abs_corr[b * c->K1 + k] = cabs(c->corr[b * c->K1 + k]);
+    }
+  }
+  /* Matsubara/residual correction, InitializePrefactors (:1375-1389). */
+  c->matsubara = (cplx *)calloc((size_t)c->nb + 1, sizeof(cplx));
+  for (int b = 0; b < c->nb; ++b) {
+    const double g = p->gamma[b], l = p->lambda[b];
+    if (g > 0) {
+      double d = 2 * l * thermal / hbar / hbar / g - l / hbar / tan(hbar * g / (2 * thermal));
+      for (int k = 1; k < c->K1; ++k)
+        d -= 4 * l * thermal / hbar / hbar * g / (pow(nu * k, 2) - pow(g, 2));
+      c->matsubara[b] = cx(d, 0.0);
+    }
+  }
+
+  const int E = N * N;
+  if (c->kind == ORACLE_BATH_DIAGONAL) {
+    /* InitializeBathCouplingOperators (:1188-1198) and
+     * Hierarchy::FillDiagonalBathOperators (hierarchy.cc:157-201). */
+    c->bath = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * N));
+    for (int k = 0; k < c->nb * N; ++k) c->bath[k] = cx(p->coupling[k], 0);
+    c->same = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    c->nextop = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    c->prevop = (cplx *)malloc(sizeof(cplx) * (size_t)(T * E));
+    for (int m = 0; m < c->nb; ++m) {
+      const cplx *V = c->bath + m * N;
+      for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) {
+          const cplx d = V[j] - V[i];
+          c->nextop[m * E + i * N + j] = cx(0, -1) * d;
+          c->same[m * E + i * N + j] = c->matsubara[m] * (d * d);
+        }
+      for (int k = 0; k < c->K1; ++k)
+        for (int i = 0; i < N; ++i)
+          for (int j = 0; j < N; ++j) {
+            const cplx cc = c->corr[m * c->K1 + k];
+            c->prevop[m * c->K1 * E + k * E + i * N + j] =
+                cx(0, -1) * (V[j] * cc - V[i] * conj(cc));
+          }
+    }
+  } else if (c->kind == ORACLE_BATH_FULL) {
+    /* Hierarchy::FillFullBathOperators (hierarchy.cc:203-216). */
+    c->bath = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    for (int k = 0; k < c->nb * E; ++k) c->bath[k] = cx(p->coupling[k], 0);
+    c->same = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    c->nextop = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    c->prevop = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+    for (int m = 0; m < c->nb; ++m)
+      for (int k = 0; k < E; ++k) {
+        c->same[m * E + k] = csqrt(c->matsubara[m]) * c->bath[m * E + k];
+        c->nextop[m * E + k] = cx(0, -1) * c->bath[m * E + k];
+        c->prevop[m * E + k] = -c->bath[m * E + k];
+      }
+  }
+  return c;
+}
+
+void oracle_destroy(oracle_ctx *c) {
+  if (!c) return;
+  free(c->mi); free(c->next); free(c->prev); free(c->tier);
+  free(c->H); free(c->Hadj); free(c->corr); free(c->abs_corr); free(c->matsubara); free(c->gamma);
+  free(c->bath); free(c->same); free(c->nextop); free(c->prevop);
+  free(c);
+}
+
+int64_t oracle_num_nodes(const oracle_ctx *c) { return c->M; }
+int oracle_num_terms(const oracle_ctx *c) { return c->T; }
+
+void oracle_get_tables(const oracle_ctx *c, int32_t *mi, int32_t *next, int32_t *prev) {
+  const size_t n = (size_t)(c->M * c->T);
+  if (mi) memcpy(mi, c->mi, n * sizeof(int32_t));
+  if (next) memcpy(next, c->next, n * sizeof(int32_t));
+  if (prev) memcpy(prev, c->prev, n * sizeof(int32_t));
+}
+
+void oracle_get_constants(const oracle_ctx *c, double *corr, double *matsubara) {
+  for (int t = 0; t < c->T; ++t) {
+    corr[2 * t] = creal(c->corr[t]);
+    corr[2 * t + 1] = cimag(c->corr[t]);
+  }
+  for (int b = 0; b < c->nb; ++b) matsubara[b] = creal(c->matsubara[b]);
+}
+
+/* ------------------------------------------------------------------------ */
+/* blas::Gemm in -DNOBLAS form (blas_wrapper.cc:11-34): C = beta*C + alpha*A*B,
+ * column-major square matrices; every blas::Hemm reduces to it (:36-56). */
+static void gemm(int N, cplx alpha, const cplx *A, const cplx *B, cplx beta, cplx *C) {
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      C[i + j * N] *= beta;
+      for (int n = 0; n < N; ++n) C[i + j * N] += alpha * (A[i + n * N] * B[j * N + n]);
+    }
+}
+/* Hemm(CblasRight, alpha, A, B) -> alpha * B * A;  Hemm(CblasLeft) -> alpha * A * B. */
+static void hemm_right(int N, cplx alpha, const cplx *A, const cplx *B, cplx beta, cplx *C) {
+  gemm(N, alpha, B, A, beta, C);
+}
+static void hemm_left(int N, cplx alpha, const cplx *A, const cplx *B, cplx beta, cplx *C) {
+  gemm(N, alpha, A, B, beta, C);
+}
+
+/* Per-node prefactors, InitializePrefactors (hierarchy_integrator.cc:1343-1466). */
+typedef struct {
+  cplx dephasing;
+  int num_next, num_prev;
+  int next_term[64], prev_term[64];
+  int32_t next_id[64], prev_id[64];
+  cplx next_pf[64], prev_row[64], prev_col[64];
+} node_prefactors;
+
+static void node_setup(const oracle_ctx *c, int64_t i, node_prefactors *np) {
+  const int T = c->T;
+  const int32_t *v = c->mi + i * T;
+  const double nu = 2 * kPi * c->kb * c->temp / c->hbar;
+  /* Dephasing: sum_t n_t nu_t; k = 0 terms decay with gamma of their bath,
+   * k >= 1 Matsubara terms with nu * k (:1365-1371). */
+  np->dephasing = 0;
+  for (int m = 0; m < T; ++m) {
+    const int drude = (m % c->K1) == 0;
+    const int k = drude ? m / c->K1 : m % c->K1;
+    const double nu_ak = drude ? c->gamma[k] : nu * k;
+    np->dephasing += cx(v[m] * nu_ak, 0);
+  }
+  np->num_next = 0;
+  np->num_prev = 0;
+  for (int t = 0; t < T; ++t) {
+    if (c->prev[i * T + t] >= 0) {
+      const int j = np->num_prev++;
+      np->prev_term[j] = t;
+      np->prev_id[j] = c->prev[i * T + t];
+      /* i n c and -i n c^*, scaled by 1/sqrt(n |c|) when normalised (:1420-1440). */
+      np->prev_row[j] = cx(0, v[t]) * c->corr[t];
+      np->prev_col[j] = cx(0, -v[t]) * conj(c->corr[t]);
+      if (c->normalized) {
+        const cplx s = 1.0 / cx(sqrt(v[t] * c->abs_corr[t]), 0);
+        np->prev_row[j] *= s;
+        np->prev_col[j] *= s;
+      }
+    }
+  }
+  for (int t = 0; t < T; ++t) {
+    if (c->next[i * T + t] >= 0) {
+      const int j = np->num_next++;
+      np->next_term[j] = t;
+      np->next_id[j] = c->next[i * T + t];
+      /* i, times sqrt((n_t + 1) |c_t|) when normalised (:1398-1411). */
+      np->next_pf[j] = cx(0, 1);
+      if (c->normalized) np->next_pf[j] *= cx(sqrt((v[t] + 1) * c->abs_corr[t]), 0);
+    }
+  }
+}
+
+/* Coupling-operator index of term t: bath_indices[t / (K+1)], the identity map
+ * (LinkHierarchyNodes, hierarchy_integrator.cc:1291-1293, :1320-1322). */
+static int term_bath(const oracle_ctx *c, int t) { return t / c->K1; }
+
+static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *out,
+                       cplx *temp) {
+  const int N = c->N, E = N * N;
+  const cplx *r = rho + i * E;
+  cplx *d = out + i * E;
+  const cplx lp = cx(0, -1.0 / c->hbar), nlp = cx(0, 1.0 / c->hbar);
+  /* DoUnitary (hierarchy_updater.h:64-70): d = -i/hbar H rho + i/hbar rho H^+. */
+  for (int k = 0; k < E; ++k) d[k] = 0;
+  hemm_right(N, lp, r, c->H, 0, d);
+  hemm_left(N, nlp, r, c->Hadj, 1, d);
+  if (c->trunc == 1) return; /* Vacuum updater: unitary part only (:206-219). */
+
+  node_prefactors np;
+  node_setup(c, i, &np);
+  /* DoDephasing (:71-75). */
+  for (int k = 0; k < E; ++k) d[k] -= np.dephasing * r[k];
+
+  if (c->kind == ORACLE_BATH_INDEPENDENT) {
+    /* IndependentBath::DoMatsubara (hierarchy_updater.cc:129-144). */
+    for (int m = 0; m < N; ++m) {
+      for (int n = 0; n < N; ++n)
+        d[m * N + n] -= r[m * N + n] * (c->matsubara[n] + c->matsubara[m]);
+      const int dd = (N + 1) * m;
+      d[dd] += 2.0 * c->matsubara[m] * r[dd];
+    }
+    /* IndependentBath::DoNext (:216-233): column m += p rho+[:, m];
+     * row m -= p rho+[m, :]. */
+    for (int j = 0; j < np.num_next; ++j) {
+      const int m = term_bath(c, np.next_term[j]);
+      const cplx *rn = rho + (int64_t)np.next_id[j] * E;
+      for (int n = 0; n < N; ++n) d[N * m + n] += np.next_pf[j] * rn[N * m + n];
+    }
+    for (int n = 0; n < N; ++n)
+      for (int j = 0; j < np.num_next; ++j) {
+        const int m = term_bath(c, np.next_term[j]);
+        const cplx *rn = rho + (int64_t)np.next_id[j] * E;
+        d[N * n + m] -= np.next_pf[j] * rn[N * n + m];
+      }
+    /* IndependentBath::DoPrevious (:235-254). */
+    for (int j = 0; j < np.num_prev; ++j) {
+      const int m = term_bath(c, np.prev_term[j]);
+      const cplx *rp = rho + (int64_t)np.prev_id[j] * E;
+      for (int n = 0; n < N; ++n) d[N * m + n] -= np.prev_col[j] * rp[N * m + n];
+    }
+    for (int n = 0; n < N; ++n)
+      for (int j = 0; j < np.num_prev; ++j) {
+        const int m = term_bath(c, np.prev_term[j]);
+        const cplx *rp = rho + (int64_t)np.prev_id[j] * E;
+        d[N * n + m] -= np.prev_row[j] * rp[N * n + m];
+      }
+  } else if (c->kind == ORACLE_BATH_DIAGONAL) {
+    /* DiagonalBath::DoMatsubara / DoNext / DoPrevious (:84-127); this updater
+     * uses the bare (unnormalised) operators whatever is_rho_normalized says. */
+    for (int m = 0; m < c->nb; ++m)
+      for (int n = 0; n < E; ++n) d[n] -= c->same[m * E + n] * r[n];
+    for (int j = 0; j < np.num_next; ++j) {
+      const cplx *op = c->nextop + term_bath(c, np.next_term[j]) * E;
+      const cplx *rn = rho + (int64_t)np.next_id[j] * E;
+      for (int n = 0; n < E; ++n) d[n] += op[n] * rn[n];
+    }
+    const int32_t *v = c->mi + i * c->T;
+    for (int j = 0; j < np.num_prev; ++j) {
+      const int t = np.prev_term[j];
+      const cplx *op = c->prevop + t * E;
+      const cplx *rp = rho + (int64_t)np.prev_id[j] * E;
+      const cplx pf = cx(v[t], 0);
+      for (int n = 0; n < E; ++n) d[n] += pf * op[n] * rp[n];
+    }
+  } else {
+    /* FullBath::DoMatsubara / DoNext / DoPrevious (:10-82). */
+    for (int m = 0; m < c->nb; ++m) {
+      const cplx *S = c->same + m * E;
+      hemm_right(N, 1, r, S, 0, temp);
+      hemm_left(N, -1, r, S, 1, temp);
+      hemm_left(N, -1, S, temp, 1, d);
+      hemm_right(N, 1, S, temp, 1, d);
+    }
+    for (int j = 0; j < np.num_next; ++j) {
+      const cplx *B = c->nextop + term_bath(c, np.next_term[j]) * E;
+      const cplx *rn = rho + (int64_t)np.next_id[j] * E;
+      hemm_right(N, cx(0, -1) * np.next_pf[j], rn, B, 1, d);
+      hemm_left(N, cx(0, 1) * np.next_pf[j], rn, B, 1, d);
+    }
+    for (int j = 0; j < np.num_prev; ++j) {
+      const cplx *B = c->prevop + term_bath(c, np.prev_term[j]) * E;
+      const cplx *rp = rho + (int64_t)np.prev_id[j] * E;
+      hemm_right(N, np.prev_row[j], rp, B, 1, d);
+      hemm_left(N, np.prev_col[j], rp, B, 1, d);
+    }
+  }
+}
+
+static void apply_all(const oracle_ctx *c, const cplx *rho, cplx *out, cplx *temp) {
+  /* FullBath's work matrix starts zeroed, as new Complex[] does (:100-102). */
+  for (int k = 0; k < c->N * c->N; ++k) temp[k] = 0;
+  for (int64_t i = 0; i < c->M; ++i) apply_node(c, i, rho, out, temp);
+}
+
+void oracle_apply(const oracle_ctx *c, const double *rho_d, double *drho_d) {
+  cplx *temp = (cplx *)malloc(sizeof(cplx) * (size_t)(c->N * c->N));
+  apply_all(c, (const cplx *)rho_d, (cplx *)drho_d, temp);
+  free(temp);
+}
+
+void oracle_initial_state(const oracle_ctx *c, const double *rho0, double *state) {
+  /* InitializeDensityMatrix (hierarchy_integrator.cc:1070-1096): node 0 gets
+   * rho(0) / prod_t sqrt(|c_t|^{n_t} n_t!), which is 1 at tier 0. */
+  const int64_t total = c->M * c->N * c->N;
+  memset(state, 0, sizeof(double) * 2 * (size_t)total);
+  memcpy(state, rho0, sizeof(double) * 2 * (size_t)(c->N * c->N));
+}
+
+/* ------------------------------------------------------------------------ */
+
+int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start_time,
+                   double end_time, double output_min_step, double *traj,
+                   double *traj_times, int64_t traj_capacity, int64_t *num_out) {
+  /* Rk4Integrate, hierarchy_integrator.cc:2578-2939. */
+  const int64_t total = c->M * c->N * c->N;
+  const int E = c->N * c->N;
+  cplx *y = (cplx *)state_d;
+  cplx *x = (cplx *)malloc(sizeof(cplx) * (size_t)total);
+  cplx *k0 = (cplx *)calloc((size_t)total, sizeof(cplx));
+  cplx *k1 = (cplx *)calloc((size_t)total, sizeof(cplx));
+  cplx *k2 = (cplx *)calloc((size_t)total, sizeof(cplx));
+  cplx *k3 = (cplx *)calloc((size_t)total, sizeof(cplx));
+  cplx *temp = (cplx *)malloc(sizeof(cplx) * (size_t)E);
+  const cplx h2 = cx(dt / 2, 0), h6 = cx(dt / 6, 0), h1 = cx(dt, 0);
+  const int output_factor = (int)ceil(output_min_step / dt); /* :2616-2617 */
+  double time_now = start_time;
+  int64_t i = -1, nout = 0;
+  while (time_now < end_time) {
+    i += 1;
+    apply_all(c, y, k0, temp);                                   /* :2709-2711 */
+    for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k0[j] * h2; /* :2715-2718 */
+    apply_all(c, x, k1, temp);
+    for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k1[j] * h2; /* :2758-2761 */
+    apply_all(c, x, k2, temp);
+    for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k2[j] * h1; /* :2777-2780 */
+    apply_all(c, x, k3, temp);
+    for (int64_t j = 0; j < total; ++j)                           /* :2822-2825 */
+      y[j] += h6 * (k0[j] + 2.0 * k1[j] + 2.0 * k2[j] + k3[j]);
+    time_now += dt;                                               /* :2856 */
+    if (output_factor > 0 && (i % output_factor) == 0) {          /* :2858 */
+      if (traj && nout < traj_capacity) {
+        memcpy(traj + 2 * nout * E, y, sizeof(cplx) * (size_t)E);
+        if (traj_times) traj_times[nout] = time_now;
+      }
+      nout++;
+    }
+  }
+  if (num_out) *num_out = nout;
+  free(x); free(k0); free(k1); free(k2); free(k3); free(temp);
+  return i + 1;
+}
+
+int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double start_time,
+                     double end_time, double tolerance, double min_dt,
+                     int64_t *accepted_out, double *final_time, double *final_dt) {
+  /* Rkf45Integrate, hierarchy_integrator.cc:1797-2573.  The step-size
+   * bookkeeping mirrors the reference: every tableau coefficient is scaled by
+   * dt once and then multiplied in place by the grow/shrink factor, and the
+   * last-step clamp permanently replaces the grow factor (:2415-2418). */
+  const int64_t total = c->M * c->N * c->N;
+  const int E = c->N * c->N;
+  cplx *y = (cplx *)state_d;
+  cplx *x = (cplx *)malloc(sizeof(cplx) * (size_t)total);
+  cplx *k[6];
+  for (int s = 0; s < 6; ++s) k[s] = (cplx *)calloc((size_t)total, sizeof(cplx));
+  cplx *temp = (cplx *)malloc(sizeof(cplx) * (size_t)E);
+  double mydt = dt0;
+  cplx dtup = 1.1, dtdn = 0.5;
+  /* Butcher tableau (:1937-1975); the fifth-order weight on k5 is 6/25. */
+  cplx b10 = 2. / 9.;
+  cplx b20 = 1. / 12., b21 = 1. / 4.;
+  cplx b30 = 69. / 128., b31 = -243. / 128., b32 = 135. / 64.;
+  cplx b40 = -17. / 12., b41 = 27. / 4., b42 = -27. / 5, b43 = 16. / 15;
+  cplx b50 = 65. / 432., b51 = -5. / 16, b52 = 13. / 16., b53 = 4. / 27., b54 = 5. / 144.;
+  cplx c50 = 1. / 9, c52 = 9. / 20, c53 = 16. / 45, c54 = 1. / 12;
+  cplx c60 = 47. / 450, c62 = 12. / 25, c63 = 32. / 225, c64 = 1. / 30, c65 = 6. / 25;
+  cplx *coef[] = {&b10, &b20, &b21, &b30, &b31, &b32, &b40, &b41, &b42, &b43,
+                  &b50, &b51, &b52, &b53, &b54, &c50, &c52, &c53, &c54,
+                  &c60, &c62, &c63, &c64, &c65};
+  const int ncoef = (int)(sizeof(coef) / sizeof(coef[0]));
+  const cplx dtc = cx(dt0, 0);
+  for (int q = 0; q < ncoef; ++q) *coef[q] *= dtc;
+  double time_now = start_time;
+  int64_t i = -1, accepted = 0;
+  while (time_now < end_time) {
+    i += 1;
+    apply_all(c, y, k[0], temp);
+    for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b10;
+    apply_all(c, x, k[1], temp);
+    for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b20 + k[1][j] * b21;
+    apply_all(c, x, k[2], temp);
+    for (int64_t j = 0; j < total; ++j)
+      x[j] = y[j] + k[0][j] * b30 + k[1][j] * b31 + k[2][j] * b32;
+    apply_all(c, x, k[3], temp);
+    for (int64_t j = 0; j < total; ++j)
+      x[j] = y[j] + k[0][j] * b40 + k[1][j] * b41 + k[2][j] * b42 + k[3][j] * b43;
+    apply_all(c, x, k[4], temp);
+    for (int64_t j = 0; j < total; ++j)
+      x[j] = y[j] + k[0][j] * b50 + k[1][j] * b51 + k[2][j] * b52 + k[3][j] * b53 +
+             k[4][j] * b54;
+    apply_all(c, x, k[5], temp);
+    /* Fourth- and fifth-order solutions and the global max-abs difference
+     * (:2317-2328, :2339-2351); x holds the fifth-order candidate. */
+    double max_diff = 0;
+    for (int64_t j = 0; j < total; ++j) {
+      const cplx y4 = y[j] + k[0][j] * c50 + k[2][j] * c52 + k[3][j] * c53 + k[4][j] * c54;
+      x[j] = y[j] + k[0][j] * c60 + k[2][j] * c62 + k[3][j] * c63 + k[4][j] * c64 +
+             k[5][j] * c65;
+      const double diff = cabs(y4 - x[j]);
+      max_diff = (diff > max_diff) ? diff : max_diff;
+    }
+    /* Accept test (:2355) taken on the step size of this attempt. */
+    if (max_diff < tolerance || mydt * creal(dtdn) < min_dt) {
+      memcpy(y, x, sizeof(cplx) * (size_t)total);
+      time_now += mydt;
+      accepted += 1;
+      int update_dt = max_diff < tolerance / 10;
+      if (time_now + mydt > end_time) {
+        update_dt = 1;
+        dtup = cx((end_time - time_now) / mydt, 0);
+      }
+      if (update_dt) {
+        mydt *= creal(dtup);
+        for (int q = 0; q < ncoef; ++q) *coef[q] *= dtup;
+      }
+    } else {
+      mydt *= creal(dtdn);
+      for (int q = 0; q < ncoef; ++q) *coef[q] *= dtdn;
+    }
+  }
+  if (accepted_out) *accepted_out = accepted;
+  if (final_time) *final_time = time_now;
+  if (final_dt) *final_dt = mydt;
+  free(x); for (int s = 0; s < 6; ++s) free(k[s]); free(temp);
+  return i + 1;
+}

@@ -1,0 +1,293 @@
+"""Python access to the oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two checkers live under oracle/:
+
+* the C restatement of the PHI path (heom_oracle.c -> _build/libheom_oracle.so);
+* the reference PHI itself, built unchanged from its sources by
+  refbuild/Makefile into _ref/ (ref_driver runs PhiParameters ->
+  HierarchyIntegrator -> Launch -> density_matrix and prints %.17g).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  The product library never calls it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import tempfile
+from ctypes import POINTER, c_double, c_int, c_int32, c_int64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "libheom_oracle.so")
+REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [
+        ("num_states", c_int), ("num_baths", c_int), ("num_matsubara", c_int),
+        ("truncation", c_int), ("bath_kind", c_int), ("normalized", c_int),
+        ("hbar", c_double), ("kb", c_double), ("temperature", c_double),
+        ("hamiltonian", POINTER(c_double)), ("gamma", POINTER(c_double)),
+        ("lambda_", POINTER(c_double)), ("coupling", POINTER(c_double)),
+    ]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB):
+        subprocess.run(["make", "-C", HERE, "_build/libheom_oracle.so"], check=True,
+                       stdout=subprocess.DEVNULL)
+    lib = ctypes.CDLL(LIB)
+    lib.oracle_node_count.restype = c_int64
+    lib.oracle_node_count.argtypes = [c_int, c_int]
+    lib.oracle_build_hierarchy.restype = c_int64
+    lib.oracle_build_hierarchy.argtypes = [c_int, c_int, c_void_p, c_int64]
+    lib.oracle_create.restype = c_void_p
+    lib.oracle_create.argtypes = [POINTER(_Problem)]
+    lib.oracle_destroy.argtypes = [c_void_p]
+    lib.oracle_num_nodes.restype = c_int64
+    lib.oracle_num_nodes.argtypes = [c_void_p]
+    lib.oracle_num_terms.restype = c_int
+    lib.oracle_num_terms.argtypes = [c_void_p]
+    lib.oracle_get_tables.argtypes = [c_void_p, c_void_p, c_void_p, c_void_p]
+    lib.oracle_get_constants.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.oracle_apply.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.oracle_initial_state.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.oracle_rk4.restype = c_int64
+    lib.oracle_rk4.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
+                               c_void_p, c_void_p, c_int64, POINTER(c_int64)]
+    lib.oracle_rkf45.restype = c_int64
+    lib.oracle_rkf45.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
+                                 c_double, POINTER(c_int64), POINTER(c_double), POINTER(c_double)]
+    _lib = lib
+    return lib
+
+
+def _colmajor(m):
+    m = np.asarray(m, dtype=np.complex128)
+    return np.ascontiguousarray(m.T).view(np.float64).reshape(-1).copy()
+
+
+def _from_colmajor(buf, n):
+    return np.asarray(buf).view(np.complex128).reshape(n, n).T.copy()
+
+
+def bath_kind(p) -> int:
+    if getattr(p, "is_full_bath_coupling", False):
+        return 2
+    if getattr(p, "is_diagonal_bath_coupling", False):
+        return 1
+    return 0
+
+
+def node_count(T: int, truncation: int) -> int:
+    return int(load().oracle_node_count(T, truncation))
+
+
+def build_hierarchy(T: int, truncation: int) -> np.ndarray:
+    """Hierarchy::ConstructI order: (M, T) multi-indices."""
+    lib = load()
+    M = node_count(T, truncation)
+    mi = np.zeros(M * max(T, 1), np.int32)
+    got = lib.oracle_build_hierarchy(T, truncation, mi.ctypes.data, M)
+    assert got == M, (got, M)
+    return mi.reshape(M, T)
+
+
+class Oracle:
+    """CPU restatement of one hierarchy instance (duck-typed PhiParameters)."""
+
+    def __init__(self, p):
+        self.lib = load()
+        n = int(p.num_states)
+        self.n = n
+        self.p = p
+        keep = []
+
+        def arr(a):
+            a = np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1))
+            keep.append(a)
+            return a.ctypes.data_as(POINTER(c_double))
+
+        pr = _Problem()
+        pr.num_states = n
+        pr.num_baths = int(p.num_bath_couplings)
+        pr.num_matsubara = int(p.num_matsubara_terms)
+        pr.truncation = int(p.hierarchy_truncation_level)
+        pr.bath_kind = bath_kind(p)
+        pr.normalized = 1 if p.is_rho_normalized else 0
+        pr.hbar = float(p.hbar)
+        pr.kb = float(p.boltzmann_constant)
+        pr.temperature = float(p.temperature)
+        pr.hamiltonian = arr(_colmajor(p.time_indepenent_hamiltonian))
+        pr.gamma = arr(p.gamma)
+        pr.lambda_ = arr(p.lambda_)
+        if pr.bath_kind == 1:
+            pr.coupling = arr(np.asarray(p.bath_coupling_op, np.float64))
+        elif pr.bath_kind == 2:
+            v = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, n, n)
+            pr.coupling = arr(np.transpose(v, (0, 2, 1)))
+        self._keep = keep
+        self.ctx = self.lib.oracle_create(ctypes.byref(pr))
+        if not self.ctx:
+            raise ValueError("oracle_create failed")
+        self.M = int(self.lib.oracle_num_nodes(self.ctx))
+        self.T = int(self.lib.oracle_num_terms(self.ctx))
+        self.rho_init = _colmajor(p.initial_density_matrix)
+
+    def __del__(self):
+        if getattr(self, "ctx", None):
+            self.lib.oracle_destroy(self.ctx)
+            self.ctx = None
+
+    @property
+    def state_len(self):
+        return 2 * self.M * self.n * self.n
+
+    def tables(self):
+        MT = self.M * self.T
+        mi, nx, pv = (np.zeros(MT, np.int32) for _ in range(3))
+        self.lib.oracle_get_tables(self.ctx, mi.ctypes.data, nx.ctypes.data, pv.ctypes.data)
+        s = (self.M, self.T)
+        return mi.reshape(s), nx.reshape(s), pv.reshape(s)
+
+    def constants(self):
+        corr = np.zeros(2 * self.T, np.float64)
+        mats = np.zeros(int(self.p.num_bath_couplings), np.float64)
+        self.lib.oracle_get_constants(self.ctx, corr.ctypes.data, mats.ctypes.data)
+        return corr.view(np.complex128), mats
+
+    def initial_state(self):
+        s = np.zeros(self.state_len, np.float64)
+        self.lib.oracle_initial_state(self.ctx, self.rho_init.ctypes.data, s.ctypes.data)
+        return s
+
+    def apply(self, state):
+        s = np.ascontiguousarray(state, np.float64)
+        out = np.zeros_like(s)
+        self.lib.oracle_apply(self.ctx, s.ctypes.data, out.ctypes.data)
+        return out
+
+    def rk4(self, state, dt, t_end, output_min_step=0.0, capacity=0, start_time=0.0):
+        s = np.ascontiguousarray(state, np.float64).copy()
+        E2 = 2 * self.n * self.n
+        traj = np.zeros(max(capacity, 1) * E2)
+        times = np.zeros(max(capacity, 1))
+        nout = c_int64()
+        steps = self.lib.oracle_rk4(self.ctx, s.ctypes.data, dt, start_time, t_end, output_min_step,
+                                    traj.ctypes.data if capacity else None,
+                                    times.ctypes.data if capacity else None, capacity,
+                                    ctypes.byref(nout))
+        k = min(nout.value, capacity)
+        rows = [_from_colmajor(traj[r * E2:(r + 1) * E2], self.n) for r in range(k)]
+        return s, int(steps), times[:k].copy(), np.array(rows)
+
+    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0):
+        s = np.ascontiguousarray(state, np.float64).copy()
+        acc = c_int64()
+        tf = c_double()
+        dtf = c_double()
+        steps = self.lib.oracle_rkf45(self.ctx, s.ctypes.data, dt0, start_time, t_end, tol, min_dt,
+                                      ctypes.byref(acc), ctypes.byref(tf), ctypes.byref(dtf))
+        return s, {"steps": int(steps), "accepted": acc.value, "final_time": tf.value,
+                   "final_dt": dtf.value}
+
+    def rho0(self, state):
+        return _from_colmajor(np.asarray(state)[:2 * self.n * self.n], self.n)
+
+
+# ---------------------------------------------------------------------------
+# The reference itself (oracle/_ref/ref_driver), driven through PHI parameter
+# files.
+
+def _fmt(x: float) -> str:
+    return repr(float(x))
+
+
+def _row(vals) -> str:
+    vals = np.asarray(vals)
+    if np.iscomplexobj(vals) and np.any(vals.imag != 0):
+        return ",".join(f"({_fmt(v.real)},{_fmt(v.imag)})" for v in vals)
+    return ",".join(_fmt(np.real(v)) for v in vals)
+
+
+def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_tol=None,
+                    rkf45_mindt=None, output_file="/dev/null") -> str:
+    """PHI parameter file (keys and layout of PhiParameters::ReadInputFile,
+    phi_parameters.cc:152-784) for a duck-typed PhiParameters."""
+    n = int(p.num_states)
+    lines = [f"OutputFile={output_file}", "verbose=-2",
+             f"hbar={_fmt(p.hbar)}", f"kB={_fmt(p.boltzmann_constant)}",
+             f"NumStates={n}", "Hamiltonian:"]
+    H = np.asarray(p.time_indepenent_hamiltonian, np.complex128)
+    lines += [_row(H[r]) for r in range(n)]
+    lines.append(f"NumCouplingTerms={int(p.num_bath_couplings)}")
+    kind = bath_kind(p)
+    if kind == 1:
+        lines.append("CorrelatedCouplingTerms:")
+        V = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, n)
+        lines += [_row(V[b]) for b in range(V.shape[0])]
+    elif kind == 2:
+        lines.append("FullBathTerms:")
+        V = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, n, n)
+        lines += [_row(V[b].T.reshape(-1)) for b in range(V.shape[0])]
+    lines += ["Gamma:", _row(p.gamma), "Lambda:", _row(p.lambda_),
+              f"Temperature={_fmt(p.temperature)}",
+              f"MatsubaraTerms={int(p.num_matsubara_terms) - 1}",
+              f"HierarchyTruncation={int(p.hierarchy_truncation_level)}",
+              f"rho_normalized={1 if p.is_rho_normalized else 0}",
+              "InitialDensityMatrix:"]
+    R = np.asarray(p.initial_density_matrix, np.complex128)
+    lines += [_row(R[r]) for r in range(n)]
+    lines.append(f"Timestep={_fmt(timestep if timestep is not None else p.timestep)}")
+    t_end = t_end if t_end is not None else p.integration_time
+    if not t_end > 0:  # the reader rejects Time <= 0 (parameter_input.cc:18-24)
+        t_end = 1e-3
+    lines.append(f"Time={_fmt(t_end)}")
+    lines.append(f"OutputMinimumTimestep={_fmt(output_min_step if output_min_step is not None else p.output_minimum_timestep)}")
+    lines.append(f"RKF45tolerance={_fmt(rkf45_tol if rkf45_tol is not None else p.rkf45_tolerance)}")
+    lines.append(f"RKF45mindt={_fmt(rkf45_mindt if rkf45_mindt is not None else p.rkf45_minimum_timestep)}")
+    return "\n".join(lines) + "\n"
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_DRIVER)
+
+
+def run_reference(p, method: str, threads: int = 1, timeout: float = 600.0, **kw):
+    """Runs the reference integrator; returns (rho_0 as N x N complex, seconds)."""
+    n = int(p.num_states)
+    with tempfile.TemporaryDirectory() as d:
+        prm = os.path.join(d, "in.prm")
+        out = os.path.join(d, "rho.txt")
+        with open(prm, "w") as f:
+            f.write(param_file_text(p, **kw))
+        subprocess.run([REF_DRIVER, "run", prm, method, str(threads), out], check=True,
+                       timeout=timeout, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+        with open(out) as f:
+            lines = f.read().split("\n")
+    secs = float(lines[0].split()[1])
+    vals = np.array([[float(x) for x in ln.split()] for ln in lines[2:2 + n * n]])
+    rho_cm = vals[:, 0] + 1j * vals[:, 1]
+    return rho_cm.reshape(n, n).T.copy(), secs
+
+
+def reference_order(p, timeout: float = 600.0) -> np.ndarray:
+    """Node order of the reference's ConstructI: (M, T) multi-indices."""
+    with tempfile.TemporaryDirectory() as d:
+        prm = os.path.join(d, "in.prm")
+        out = os.path.join(d, "order.txt")
+        with open(prm, "w") as f:
+            f.write(param_file_text(p))
+        subprocess.run([REF_DRIVER, "order", prm, out], check=True, timeout=timeout,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
+        rows = [ln.split() for ln in open(out).read().strip().split("\n")]
+    return np.array([[int(x) for x in r] for r in rows], dtype=np.int32)

@@ -1,0 +1,37 @@
+// heom_kernels.h -- launch interface of the HEOM stage kernels (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "heom_device.cuh"
+
+namespace phi {
+
+enum StageMode : int { kModeApply = 0, kModeRk4 = 1, kModeRkf45 = 2 };
+
+// Everything one stage launch needs; pointers are device pointers.
+struct StageLaunch {
+  HeomConsts c;
+  int mode = kModeApply;
+  int stage = 0;
+  int grid = 1;
+  const double2 *x = nullptr;   // stage input
+  double2 *out = nullptr;       // apply output / next stage input
+  double2 *y = nullptr;         // RK4 state
+  double2 *acc = nullptr;       // RK4 accumulator
+  double a_next = 0.0;          // RK4: X_{s+1} = y + a_next k_s
+  double w_acc = 0.0;           // RK4: accumulator weight of k_s
+  Rk4Ctl *rk4 = nullptr;
+  double2 *traj = nullptr;      // RK4 rho_0 trajectory rows
+  double2 *k[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RKF45 k0..k4
+  double2 *ybuf[2] = {nullptr, nullptr};                          // RKF45 state ping-pong
+  Rkf45Ctl *ctl = nullptr;
+};
+
+int choose_group(int N);
+size_t stage_smem_bytes(int N, int T, int kind);
+int stage_grid(const HeomConsts &c, int num_sms);
+cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream);
+cudaError_t launch_rkf45_control(Rkf45Ctl *ctl, cudaStream_t stream);
+
+}  // namespace phi

@@ -1,0 +1,427 @@
+// phi_capi.cu -- the C ABI (include/phi_b200.h): one hierarchy instance on
+// one GPU.  Host-side setup restates the constants PHI computes in
+// HierarchyIntegrator::Initialize / InitializePrefactors
+// (hierarchy_integrator.cc:376-594, :1343-1466); everything per node lives on
+// the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/phi_b200.h"
+#include "heom_device.cuh"
+#include "heom_internal.h"
+#include "heom_kernels.h"
+#include "phi_context.h"
+
+using phi::DeviceBuffer;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+// hierarchy_node.h:7
+constexpr double kPi = 3.14159265358979323846264338327950288419716939937510;
+
+int fail(phi_ctx *ctx, int code, const std::string &msg) {
+  if (ctx) ctx->error = msg;
+  else g_create_error = msg;
+  return code;
+}
+
+int cuda_fail(phi_ctx *ctx, cudaError_t e, const char *where) {
+  return fail(ctx, PHI_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define PHI_CUDA(ctx, call)                                   \
+  do {                                                        \
+    cudaError_t e_ = (call);                                  \
+    if (e_ != cudaSuccess) return cuda_fail((ctx), e_, #call); \
+  } while (0)
+
+template <class T>
+cudaError_t upload(DeviceBuffer &buf, const std::vector<T> &v, cudaStream_t s) {
+  cudaError_t e = buf.alloc(std::max<size_t>(v.size() * sizeof(T), 16));
+  if (e != cudaSuccess) return e;
+  if (v.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(buf.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+bool is_hermitian(const double *m, int N, double *scale_out) {
+  double scale = 0;
+  for (int k = 0; k < N * N; ++k) scale = std::max(scale, std::hypot(m[2 * k], m[2 * k + 1]));
+  const double tol = 1e-12 * std::max(scale, 1e-300);
+  for (int r = 0; r < N; ++r)
+    for (int c = 0; c < N; ++c) {
+      const double *a = m + 2 * (r + c * N), *b = m + 2 * (c + r * N);
+      if (std::fabs(a[0] - b[0]) > tol || std::fabs(a[1] + b[1]) > tol) return false;
+    }
+  if (scale_out) *scale_out = scale;
+  return true;
+}
+
+}  // namespace
+
+namespace phi {
+
+// Builds the per-term / per-element constant tables and the device copy of
+// the problem (see HeomConsts).
+int setup_constants(phi_ctx *ctx) {
+  const phi_problem_desc &d = ctx->desc;
+  const int N = d.num_states, nb = d.num_baths, K1 = d.num_matsubara_terms;
+  const int T = nb * K1, L = d.truncation_level - 1, E = N * N;
+  const double hbar = d.hbar;
+  const double thermal = d.boltzmann_constant * d.temperature;
+  const double nu = 2 * kPi * thermal / hbar;
+
+  // Correlation-function constants c_t, t = b*(K+1) + k
+  // (hierarchy_integrator.cc:427-473).
+  std::vector<std::complex<double>> corr(T, 0.0);
+  std::vector<double> abs_corr(T, 0.0), rates(T, 0.0), delta(nb, 0.0);
+  for (int b = 0; b < nb; ++b) {
+    const double g = ctx->gamma[b], l = ctx->lambda[b];
+    if (g > 0) {
+      const double a = g * l / hbar;
+      corr[b * K1] = std::complex<double>(a / std::tan(g * hbar / (2 * thermal)), -a);
+      for (int k = 1; k < K1; ++k)
+        corr[b * K1 + k] = 4 * l * g * thermal / hbar / hbar * (nu * k) /
+                           (std::pow(nu * k, 2) - std::pow(g, 2));
+      // Matsubara/residual correction (:1375-1389).
+      double dl = 2 * l * thermal / hbar / hbar / g - l / hbar / std::tan(hbar * g / (2 * thermal));
+      for (int k = 1; k < K1; ++k) dl -= 4 * l * thermal / hbar / hbar * g / (std::pow(nu * k, 2) - std::pow(g, 2));
+      delta[b] = dl;
+    }
+    for (int k = 0; k < K1; ++k) abs_corr[b * K1 + k] = std::abs(corr[b * K1 + k]);
+    // Dephasing rate of each term (:1362-1371): gamma for k = 0, nu*k else.
+    for (int k = 0; k < K1; ++k) rates[b * K1 + k] = k == 0 ? g : nu * k;
+  }
+  ctx->corr = corr;
+  ctx->delta = delta;
+
+  const bool vacuum = d.truncation_level == 1;
+  const bool normalized = d.normalized != 0;
+  if (!vacuum && d.bath_kind != PHI_BATH_DIAGONAL && normalized) {
+    for (int t = 0; t < T; ++t)
+      if (!(abs_corr[t] > 0))
+        return fail(ctx, PHI_E_INVALID,
+                    "correlation constant |c_" + std::to_string(t) +
+                        "| is zero (gamma or lambda <= 0): the normalised hierarchy is undefined");
+  }
+  // Prefactor magnitudes for n_t = 0..L+1 (:1393-1441).
+  const int W = L + 2;
+  std::vector<double> sq_next((size_t)T * W, 1.0), sq_prev((size_t)T * W, 0.0);
+  for (int t = 0; t < T; ++t)
+    for (int n = 0; n < W; ++n) {
+      sq_next[(size_t)t * W + n] = normalized ? std::sqrt((n + 1) * abs_corr[t]) : 1.0;
+      sq_prev[(size_t)t * W + n] =
+          normalized ? (n > 0 ? std::sqrt(n / abs_corr[t]) : 0.0) : (double)n;
+    }
+
+  // Coupling map.  IndependentBath: term t couples to site s_{t/(K+1)};
+  // DiagonalBath / FullBath: to bath operator t/(K+1)
+  // (LinkHierarchyNodes, :1291-1293 and :1320-1322).
+  std::vector<int32_t> term_site(T), site_ptr(N + 1, 0), site_terms(T);
+  std::vector<double> site_delta(N, 0.0);
+  for (int t = 0; t < T; ++t) {
+    const int b = t / K1;
+    term_site[t] = d.bath_kind == PHI_BATH_INDEPENDENT ? ctx->bath_sites[b] : b;
+  }
+  if (d.bath_kind == PHI_BATH_INDEPENDENT) {
+    for (int t = 0; t < T; ++t) site_ptr[term_site[t] + 1]++;
+    for (int s = 0; s < N; ++s) site_ptr[s + 1] += site_ptr[s];
+    std::vector<int32_t> fill(site_ptr.begin(), site_ptr.end() - 1);
+    for (int t = 0; t < T; ++t) site_terms[fill[term_site[t]]++] = t;
+    for (int b = 0; b < nb; ++b) site_delta[ctx->bath_sites[b]] += delta[b];
+  }
+  // Element-wise Matsubara factor: IndependentBath::DoMatsubara
+  // (hierarchy_updater.cc:129-144) and DiagonalBath same operator
+  // (hierarchy.cc:167-168); FullBath and Vacuum use none here.
+  std::vector<double> mats_elem(E, 0.0);
+  if (!vacuum) {
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double f = 0.0;
+        if (d.bath_kind == PHI_BATH_INDEPENDENT) {
+          if (i != j) f = site_delta[i] + site_delta[j];
+        } else if (d.bath_kind == PHI_BATH_DIAGONAL) {
+          for (int b = 0; b < nb; ++b) {
+            const double dv = ctx->coupling[(size_t)b * N + i] - ctx->coupling[(size_t)b * N + j];
+            f += delta[b] * dv * dv;
+          }
+        }
+        mats_elem[i + j * N] = f;
+      }
+  }
+  std::vector<uint8_t> pi, pj;
+  for (int j = 0; j < N; ++j)
+    for (int i = 0; i <= j; ++i) {
+      pi.push_back((uint8_t)i);
+      pj.push_back((uint8_t)j);
+    }
+  std::vector<double2> H(E), corr2(T);
+  for (int k = 0; k < E; ++k) H[k] = make_double2(ctx->hamiltonian[2 * k], ctx->hamiltonian[2 * k + 1]);
+  for (int t = 0; t < T; ++t) corr2[t] = make_double2(corr[t].real(), corr[t].imag());
+
+  cudaStream_t s = ctx->stream;
+  auto &cb = ctx->cbuf;
+  cudaError_t e = cudaSuccess;
+  auto chk = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
+  chk(upload(cb.H, H, s));
+  chk(upload(cb.corr, corr2, s));
+  chk(upload(cb.nu, rates, s));
+  chk(upload(cb.sq_next, sq_next, s));
+  chk(upload(cb.sq_prev, sq_prev, s));
+  chk(upload(cb.term_site, term_site, s));
+  chk(upload(cb.site_ptr, site_ptr, s));
+  chk(upload(cb.site_terms, site_terms, s));
+  chk(upload(cb.mats_elem, mats_elem, s));
+  chk(upload(cb.bath_V, ctx->coupling, s));
+  chk(upload(cb.mats_bath, delta, s));
+  chk(upload(cb.pair_i, pi, s));
+  chk(upload(cb.pair_j, pj, s));
+  chk(cudaStreamSynchronize(s));
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "constant upload");
+
+  HeomConsts &c = ctx->c;
+  c.N = N;
+  c.T = T;
+  c.K1 = K1;
+  c.nb = nb;
+  c.L = L;
+  c.kind = d.bath_kind;
+  c.vacuum = vacuum ? 1 : 0;
+  c.M = ctx->hier.M;
+  c.inv_hbar = 1.0 / hbar;
+  c.mi = ctx->hier.mi.as<uint8_t>();
+  c.next = ctx->hier.next.as<int32_t>();
+  c.prev = ctx->hier.prev.as<int32_t>();
+  c.H = cb.H.as<double2>();
+  c.corr = cb.corr.as<double2>();
+  c.nu = cb.nu.as<double>();
+  c.sq_next = cb.sq_next.as<double>();
+  c.sq_prev = cb.sq_prev.as<double>();
+  c.term_site = cb.term_site.as<int32_t>();
+  c.site_ptr = cb.site_ptr.as<int32_t>();
+  c.site_terms = cb.site_terms.as<int32_t>();
+  c.mats_elem = cb.mats_elem.as<double>();
+  c.bath_V = cb.bath_V.as<double>();
+  c.mats_bath = cb.mats_bath.as<double>();
+  c.pair_i = cb.pair_i.as<uint8_t>();
+  c.pair_j = cb.pair_j.as<uint8_t>();
+  return PHI_OK;
+}
+
+}  // namespace phi
+
+// --------------------------------------------------------------------------
+
+extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
+  if (!out) return fail(nullptr, PHI_E_INVALID, "out is NULL");
+  *out = nullptr;
+  if (!desc) return fail(nullptr, PHI_E_INVALID, "desc is NULL");
+  const phi_problem_desc &d = *desc;
+  const int N = d.num_states;
+  if (N < 1 || N > phi::kMaxStates) return fail(nullptr, PHI_E_INVALID, "num_states must be in [1, 64]");
+  if (d.num_baths < 1) return fail(nullptr, PHI_E_INVALID, "num_baths must be >= 1");
+  if (d.num_matsubara_terms < 1) return fail(nullptr, PHI_E_INVALID, "num_matsubara_terms (K+1) must be >= 1");
+  if (d.truncation_level < 1) return fail(nullptr, PHI_E_INVALID, "truncation_level must be >= 1");
+  const long long T = (long long)d.num_baths * d.num_matsubara_terms;
+  if (T > phi::kMaxTerms) return fail(nullptr, PHI_E_INVALID, "num_baths * (K+1) must be <= 64");
+  if (d.truncation_level - 1 > phi::kMaxTier) return fail(nullptr, PHI_E_INVALID, "truncation_level must be <= 251");
+  if (d.bath_kind < PHI_BATH_INDEPENDENT || d.bath_kind > PHI_BATH_FULL)
+    return fail(nullptr, PHI_E_INVALID, "unknown bath_kind");
+  if (d.precision != PHI_PREC_FP64 && d.precision != PHI_PREC_MIXED)
+    return fail(nullptr, PHI_E_INVALID, "unknown precision");
+  if (!d.hamiltonian || !d.initial_density_matrix || !d.gamma || !d.lambda)
+    return fail(nullptr, PHI_E_INVALID, "hamiltonian, initial_density_matrix, gamma and lambda are required");
+  if (!(d.hbar > 0) || !(d.boltzmann_constant > 0) || !(d.temperature > 0))
+    return fail(nullptr, PHI_E_INVALID, "hbar, boltzmann_constant and temperature must be positive");
+  if (d.bath_kind != PHI_BATH_INDEPENDENT && !d.coupling)
+    return fail(nullptr, PHI_E_INVALID, "diagonal and full baths need coupling operators");
+  for (int k = 0; k < 2 * N * N; ++k)
+    if (!std::isfinite(d.hamiltonian[k]) || !std::isfinite(d.initial_density_matrix[k]))
+      return fail(nullptr, PHI_E_INVALID, "non-finite value in the Hamiltonian or initial density matrix");
+  if (!is_hermitian(d.initial_density_matrix, N, nullptr))
+    return fail(nullptr, PHI_E_INVALID,
+                "initial density matrix is not Hermitian (PHI's hierarchy keeps every ADO Hermitian)");
+
+  std::unique_ptr<phi_ctx> ctx(new phi_ctx());
+  ctx->desc = d;
+  ctx->hamiltonian.assign(d.hamiltonian, d.hamiltonian + 2 * N * N);
+  ctx->rho_init.assign(d.initial_density_matrix, d.initial_density_matrix + 2 * N * N);
+  ctx->gamma.assign(d.gamma, d.gamma + d.num_baths);
+  ctx->lambda.assign(d.lambda, d.lambda + d.num_baths);
+  if (d.bath_kind == PHI_BATH_DIAGONAL) ctx->coupling.assign(d.coupling, d.coupling + (size_t)d.num_baths * N);
+  if (d.bath_kind == PHI_BATH_FULL) {
+    ctx->coupling.assign(d.coupling, d.coupling + (size_t)d.num_baths * N * N);
+    for (int b = 0; b < d.num_baths; ++b)
+      for (int r = 0; r < N; ++r)
+        for (int c = 0; c < N; ++c)
+          if (ctx->coupling[(size_t)b * N * N + r + c * N] != ctx->coupling[(size_t)b * N * N + c + r * N])
+            return fail(nullptr, PHI_E_INVALID, "full bath coupling operators must be symmetric");
+  }
+  ctx->bath_sites.resize(d.num_baths);
+  if (d.bath_kind == PHI_BATH_INDEPENDENT) {
+    if (d.bath_sites) {
+      for (int b = 0; b < d.num_baths; ++b) {
+        if (d.bath_sites[b] < 0 || d.bath_sites[b] >= N)
+          return fail(nullptr, PHI_E_INVALID, "bath_sites entries must be in [0, num_states)");
+        ctx->bath_sites[b] = d.bath_sites[b];
+      }
+    } else {
+      if (d.num_baths != N && d.truncation_level > 1)
+        return fail(nullptr, PHI_E_INVALID,
+                    "independent baths without bath_sites need num_baths == num_states "
+                    "(PHI couples bath j to |j><j|)");
+      for (int b = 0; b < d.num_baths; ++b) ctx->bath_sites[b] = b < N ? b : 0;
+    }
+  }
+  ctx->desc.hamiltonian = nullptr;
+  ctx->desc.initial_density_matrix = nullptr;
+  ctx->desc.gamma = ctx->desc.lambda = ctx->desc.coupling = nullptr;
+  ctx->desc.bath_sites = nullptr;
+
+  cudaError_t e = cudaSetDevice(d.device);
+  if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+  e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, d.device);
+
+  ctx->hier.budget = d.max_nodes;
+  std::string err;
+  int rc = phi::build_hierarchy_device((int)T, d.truncation_level - 1, &ctx->hier, &err, ctx->stream);
+  if (rc != 0) {
+    const int code = rc == 2 ? PHI_E_OOM : rc == 3 ? PHI_E_BUDGET : rc == 7 ? PHI_E_CUDA : PHI_E_INVALID;
+    return fail(nullptr, code, err);
+  }
+  rc = phi::setup_constants(ctx.get());
+  if (rc != PHI_OK) {
+    g_create_error = ctx->error;
+    return rc;
+  }
+  ctx->grid = phi::stage_grid(ctx->c, ctx->num_sms);
+  const size_t state_bytes = (size_t)ctx->hier.M * N * N * sizeof(double2);
+  e = ctx->y.alloc(state_bytes);
+  if (e != cudaSuccess) return fail(nullptr, PHI_E_OOM, "state allocation failed: " + std::to_string(state_bytes) + " bytes");
+  // InitializeDensityMatrix (hierarchy_integrator.cc:1070-1096): rho(0) in
+  // node 0, scaled by prod sqrt(|c|^n n!) = 1 at tier 0; zero elsewhere.
+  e = cudaMemsetAsync(ctx->y.ptr, 0, state_bytes, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
+                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("initial state: ") + cudaGetErrorString(e));
+  ctx->time = 0.0;
+  *out = ctx.release();
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_destroy(phi_ctx *ctx) {
+  if (!ctx) return PHI_OK;
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  ctx->release_graphs();
+  cudaStream_t s = ctx->stream;
+  delete ctx;
+  if (s) cudaStreamDestroy(s);
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
+                            int32_t *num_states) {
+  if (!ctx) return PHI_E_INVALID;
+  if (num_nodes) *num_nodes = ctx->hier.M;
+  if (num_terms) *num_terms = ctx->hier.T;
+  if (num_states) *num_states = ctx->desc.num_states;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_node_table(const phi_ctx *cctx, int32_t *multi_index, int32_t *next,
+                                      int32_t *prev) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx) return PHI_E_INVALID;
+  const size_t n = (size_t)ctx->hier.M * ctx->hier.T;
+  if (multi_index) {
+    std::vector<uint8_t> tmp(n);
+    PHI_CUDA(ctx, cudaMemcpyAsync(tmp.data(), ctx->hier.mi.ptr, n, cudaMemcpyDeviceToHost, ctx->stream));
+    PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (size_t i = 0; i < n; ++i) multi_index[i] = tmp[i];
+  }
+  if (next) PHI_CUDA(ctx, cudaMemcpyAsync(next, ctx->hier.next.ptr, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  if (prev) PHI_CUDA(ctx, cudaMemcpyAsync(prev, ctx->hier.prev.ptr, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_set_state(phi_ctx *ctx, const double *state) {
+  if (!ctx || !state) return PHI_E_INVALID;
+  PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, state, ctx->state_bytes(), cudaMemcpyHostToDevice, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_state(const phi_ctx *cctx, double *state) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !state) return PHI_E_INVALID;
+  PHI_CUDA(ctx, cudaMemcpyAsync(state, ctx->y.ptr, ctx->state_bytes(), cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_rho0(const phi_ctx *cctx, double *rho0) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !rho0) return PHI_E_INVALID;
+  const size_t b = (size_t)ctx->desc.num_states * ctx->desc.num_states * sizeof(double2);
+  PHI_CUDA(ctx, cudaMemcpyAsync(rho0, ctx->y.ptr, b, cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream) {
+  if (!ctx || !d_in || !d_out) return PHI_E_INVALID;
+  phi::StageLaunch L;
+  L.c = ctx->c;
+  L.mode = phi::kModeApply;
+  L.grid = ctx->grid;
+  L.x = static_cast<const double2 *>(d_in);
+  L.out = static_cast<double2 *>(d_out);
+  PHI_CUDA(ctx, phi::launch_stage(L, static_cast<cudaStream_t>(stream)));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_apply(phi_ctx *ctx, const double *in, double *out) {
+  if (!ctx || !in || !out) return PHI_E_INVALID;
+  int rc = ctx->ensure_work(1);
+  if (rc != PHI_OK) return rc;
+  const size_t b = ctx->state_bytes();
+  PHI_CUDA(ctx, cudaMemcpyAsync(ctx->xa.ptr, in, b, cudaMemcpyHostToDevice, ctx->stream));
+  rc = phi_gpu_apply_device(ctx, ctx->xa.ptr, ctx->xb.ptr, ctx->stream);
+  if (rc != PHI_OK) return rc;
+  PHI_CUDA(ctx, cudaMemcpyAsync(out, ctx->xb.ptr, b, cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_time(const phi_ctx *ctx, double *time) {
+  if (!ctx || !time) return PHI_E_INVALID;
+  *time = ctx->time;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_set_time(phi_ctx *ctx, double time) {
+  if (!ctx) return PHI_E_INVALID;
+  ctx->time = time;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len) {
+  if (!buf || len == 0) return PHI_E_INVALID;
+  const std::string &s = ctx ? ctx->error : g_create_error;
+  std::snprintf(buf, len, "%s", s.c_str());
+  return PHI_OK;
+}

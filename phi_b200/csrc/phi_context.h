@@ -1,0 +1,67 @@
+// phi_context.h -- the opaque phi_ctx of the C ABI (internal).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <complex>
+#include <string>
+#include <vector>
+
+#include "../../include/phi_b200.h"
+#include "heom_device.cuh"
+#include "heom_internal.h"
+
+// Device copies of the per-term / per-element constants (HeomConsts points here).
+struct PhiConstBuffers {
+  phi::DeviceBuffer H, corr, nu, sq_next, sq_prev, term_site, site_ptr, site_terms,
+      mats_elem, bath_V, mats_bath, pair_i, pair_j;
+};
+
+struct phi_ctx {
+  phi_problem_desc desc{};             // scalar fields; array pointers cleared
+  std::vector<double> hamiltonian;     // 2*N*N
+  std::vector<double> rho_init;        // 2*N*N
+  std::vector<double> gamma, lambda;   // num_baths
+  std::vector<double> coupling;        // diagonal / full operators
+  std::vector<int32_t> bath_sites;     // independent: site of each bath
+  std::vector<std::complex<double>> corr;
+  std::vector<double> delta;
+
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  int grid = 1;
+  phi::DeviceHierarchy hier;
+  PhiConstBuffers cbuf;
+  phi::HeomConsts c{};
+
+  // State and integrator work space (node-major, complex128).
+  phi::DeviceBuffer y;         // current state
+  phi::DeviceBuffer y_alt;     // RKF45 candidate state
+  phi::DeviceBuffer xa, xb;    // stage inputs (ping-pong)
+  phi::DeviceBuffer acc;       // RK4 accumulator
+  phi::DeviceBuffer kbuf[5];   // RKF45 k0..k4
+  phi::DeviceBuffer ctl;       // Rkf45Ctl / Rk4Ctl
+  phi::DeviceBuffer traj;      // rho_0 rows
+  int work_level = 0;          // 1: xa/xb, 2: + acc, 3: + RKF45 buffers
+
+  // Captured step graphs.
+  cudaGraphExec_t rk4_graph = nullptr;
+  int rk4_graph_steps = 0;
+  double rk4_graph_dt = 0.0;
+  void *rk4_graph_traj = nullptr;
+  cudaGraphExec_t rkf45_graph = nullptr;
+  int rkf45_graph_steps = 0;
+
+  double time = 0.0;
+  std::string error;
+
+  size_t state_bytes() const {
+    return (size_t)hier.M * desc.num_states * desc.num_states * sizeof(double2);
+  }
+  int ensure_work(int level);
+  void release_graphs();
+};
+
+namespace phi {
+int setup_constants(phi_ctx *ctx);
+}

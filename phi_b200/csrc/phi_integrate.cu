@@ -1,0 +1,298 @@
+// phi_integrate.cu -- RK4 and RKF45 drivers: fused stage kernels replayed
+// from captured CUDA graphs.
+//
+// RK4 (Rk4Integrate, hierarchy_integrator.cc:2578-2939) keeps four state-size
+// buffers: y, acc, and the stage inputs X_a / X_b.  Stage s computes
+// k_s = L(X_s) and in the same kernel writes X_{s+1} = y + a_s k_s and the
+// accumulator acc (= y + dt/6 k0 + dt/3 k1 + dt/3 k2, then y = acc + dt/6 k3).
+//
+// RKF45 (Rkf45Integrate, :1797-2573) keeps y, the candidate y5, k0..k4 and the
+// stage inputs.  The accept/reject decision and the step-size update run on
+// the device (rkf45_control_kernel) so a captured graph of many steps needs
+// no host round trip; the host polls a done flag between graph launches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/phi_b200.h"
+#include "heom_kernels.h"
+#include "phi_context.h"
+
+namespace {
+
+int cuda_err(phi_ctx *ctx, cudaError_t e, const char *where) {
+  ctx->error = std::string(where) + ": " + cudaGetErrorString(e);
+  return PHI_E_CUDA;
+}
+
+#define PHI_CK(call)                                              \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) return cuda_err(ctx, e_, #call);       \
+  } while (0)
+
+constexpr int kGraphSteps = 16;
+
+}  // namespace
+
+int phi_ctx::ensure_work(int level) {
+  const size_t b = state_bytes();
+  auto alloc = [&](phi::DeviceBuffer &buf) -> bool {
+    if (buf.ptr) return true;
+    return buf.alloc(b) == cudaSuccess;
+  };
+  bool ok = true;
+  if (level >= 1) ok = ok && alloc(xa) && alloc(xb);
+  if (level >= 2) ok = ok && alloc(acc);
+  if (level >= 3) {
+    ok = ok && alloc(y_alt);
+    for (auto &k : kbuf) ok = ok && alloc(k);
+  }
+  if (ok && !ctl.ptr) ok = ctl.alloc(std::max(sizeof(phi::Rkf45Ctl), sizeof(phi::Rk4Ctl))) == cudaSuccess;
+  if (!ok) {
+    error = "work-space allocation failed (" + std::to_string(b) + " bytes per buffer)";
+    return PHI_E_OOM;
+  }
+  work_level = std::max(work_level, level);
+  return PHI_OK;
+}
+
+void phi_ctx::release_graphs() {
+  if (rk4_graph) cudaGraphExecDestroy(rk4_graph);
+  if (rkf45_graph) cudaGraphExecDestroy(rkf45_graph);
+  rk4_graph = nullptr;
+  rkf45_graph = nullptr;
+}
+
+namespace {
+
+// Enqueues one RK4 step (four fused stage kernels).
+cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, cudaStream_t s) {
+  phi::StageLaunch L;
+  L.c = ctx->c;
+  L.mode = phi::kModeRk4;
+  L.grid = ctx->grid;
+  L.y = ctx->y.as<double2>();
+  L.acc = ctx->acc.as<double2>();
+  L.rk4 = ctx->ctl.as<phi::Rk4Ctl>();
+  L.traj = traj;
+  double2 *xa = ctx->xa.as<double2>(), *xb = ctx->xb.as<double2>();
+  const double a[4] = {dt / 2, dt / 2, dt, 0.0};
+  const double w[4] = {dt / 6, dt / 3, dt / 3, dt / 6};
+  const double2 *in[4] = {L.y, xa, xb, xa};
+  double2 *outb[4] = {xa, xb, xa, nullptr};
+  for (int st = 0; st < 4; ++st) {
+    L.stage = st;
+    L.x = in[st];
+    L.out = outb[st];
+    L.a_next = a[st];
+    L.w_acc = w[st];
+    cudaError_t e = phi::launch_stage(L, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
+  phi::StageLaunch L;
+  L.c = ctx->c;
+  L.mode = phi::kModeRkf45;
+  L.grid = ctx->grid;
+  L.ctl = ctx->ctl.as<phi::Rkf45Ctl>();
+  L.ybuf[0] = ctx->y.as<double2>();
+  L.ybuf[1] = ctx->y_alt.as<double2>();
+  for (int i = 0; i < 5; ++i) L.k[i] = ctx->kbuf[i].as<double2>();
+  double2 *xa = ctx->xa.as<double2>(), *xb = ctx->xb.as<double2>();
+  const double2 *in[6] = {nullptr, xa, xb, xa, xb, xa};
+  double2 *outb[6] = {xa, xb, xa, xb, xa, nullptr};
+  for (int st = 0; st < 6; ++st) {
+    L.stage = st;
+    L.x = in[st];
+    L.out = outb[st];
+    cudaError_t e = phi::launch_stage(L, s);
+    if (e != cudaSuccess) return e;
+  }
+  return phi::launch_rkf45_control(L.ctl, s);
+}
+
+template <class F>
+cudaError_t capture(cudaStream_t s, F &&body, cudaGraphExec_t *exec) {
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  cudaError_t eb = body();
+  e = cudaStreamEndCapture(s, &graph);
+  if (eb != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    return eb;
+  }
+  if (e != cudaSuccess) return e;
+  e = cudaGraphInstantiate(exec, graph, 0);
+  cudaGraphDestroy(graph);
+  return e;
+}
+
+}  // namespace
+
+extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min_step,
+                           double *traj, double *times, int64_t capacity, int64_t *num_steps,
+                           int64_t *num_out) {
+  if (!ctx) return PHI_E_INVALID;
+  if (!(dt > 0) || !std::isfinite(t_end)) {
+    ctx->error = "rk4: dt must be positive and t_end finite";
+    return PHI_E_INVALID;
+  }
+  int rc = ctx->ensure_work(2);
+  if (rc != PHI_OK) return rc;
+  // Step count and output times: the reference's loop
+  // `while (time_now < end_time) { ...; time_now += dt_f_; }` (:2682, :2856).
+  const long long out_factor = (long long)std::ceil(output_min_step / dt);
+  std::vector<double> out_times;
+  long long steps = 0;
+  double t = ctx->time;
+  while (t < t_end) {
+    t += dt;
+    if (out_factor > 0 && steps % out_factor == 0) out_times.push_back(t);
+    ++steps;
+    if (steps > (1ll << 40)) {
+      ctx->error = "rk4: step count overflow";
+      return PHI_E_INVALID;
+    }
+  }
+  const long long rows = std::min<long long>((long long)out_times.size(), traj ? capacity : 0);
+  double2 *dtraj = nullptr;
+  if (rows > 0) {
+    const size_t need = (size_t)rows * ctx->desc.num_states * ctx->desc.num_states * sizeof(double2);
+    if (ctx->traj.bytes < need && ctx->traj.alloc(need) != cudaSuccess) {
+      ctx->error = "rk4: trajectory allocation failed";
+      return PHI_E_OOM;
+    }
+    dtraj = ctx->traj.as<double2>();
+  }
+  phi::Rk4Ctl hc{};
+  hc.step = 0;
+  hc.out_factor = out_factor;
+  hc.capacity = rows;
+  hc.nout = 0;
+  PHI_CK(cudaMemcpyAsync(ctx->ctl.ptr, &hc, sizeof(hc), cudaMemcpyHostToDevice, ctx->stream));
+
+  // Replay a graph of kGraphSteps steps; the tail runs as direct launches.
+  if (steps >= kGraphSteps &&
+      (!ctx->rk4_graph || ctx->rk4_graph_dt != dt || ctx->rk4_graph_traj != (void *)dtraj)) {
+    if (ctx->rk4_graph) cudaGraphExecDestroy(ctx->rk4_graph);
+    ctx->rk4_graph = nullptr;
+    PHI_CK(capture(ctx->stream, [&]() {
+      for (int i = 0; i < kGraphSteps; ++i) {
+        cudaError_t e = enqueue_rk4_step(ctx, dt, dtraj, ctx->stream);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    }, &ctx->rk4_graph));
+    ctx->rk4_graph_dt = dt;
+    ctx->rk4_graph_traj = dtraj;
+  }
+  long long done = 0;
+  while (steps - done >= kGraphSteps) {
+    PHI_CK(cudaGraphLaunch(ctx->rk4_graph, ctx->stream));
+    done += kGraphSteps;
+  }
+  for (; done < steps; ++done) PHI_CK(enqueue_rk4_step(ctx, dt, dtraj, ctx->stream));
+  if (rows > 0) {
+    PHI_CK(cudaMemcpyAsync(traj, dtraj, (size_t)rows * ctx->desc.num_states * ctx->desc.num_states * sizeof(double2),
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  PHI_CK(cudaStreamSynchronize(ctx->stream));
+  if (times)
+    for (long long r = 0; r < std::min<long long>((long long)out_times.size(), capacity); ++r) times[r] = out_times[r];
+  ctx->time = t;
+  if (num_steps) *num_steps = steps;
+  if (num_out) *num_out = (int64_t)out_times.size();
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
+                             int64_t max_steps, phi_rkf45_stats *stats) {
+  if (!ctx) return PHI_E_INVALID;
+  if (!(dt0 > 0) || !(tol > 0) || !(min_dt > 0) || !std::isfinite(t_end)) {
+    ctx->error = "rkf45: dt0, tol and min_dt must be positive and t_end finite";
+    return PHI_E_INVALID;
+  }
+  int rc = ctx->ensure_work(3);
+  if (rc != PHI_OK) return rc;
+  phi::Rkf45Ctl hc{};
+  hc.time = ctx->time;
+  hc.end_time = t_end;
+  hc.dt = dt0;
+  hc.tol = tol;
+  hc.min_dt = min_dt;
+  hc.dtup = 1.1;
+  hc.dtdn = 0.5;
+  // Butcher tableau of Rkf45Integrate (:1937-1975), each entry scaled by dt0.
+  const double tab[24] = {2. / 9.,   1. / 12.,  1. / 4.,   69. / 128., -243. / 128., 135. / 64.,
+                          -17. / 12., 27. / 4.,  -27. / 5,  16. / 15,   65. / 432.,   -5. / 16,
+                          13. / 16.,  4. / 27.,  5. / 144., 1. / 9,     9. / 20,      16. / 45,
+                          1. / 12,    47. / 450, 12. / 25,  32. / 225,  1. / 30,      6. / 25};
+  for (int q = 0; q < 24; ++q) hc.coef[q] = tab[q] * dt0;
+  hc.max_error = 0.0;
+  hc.err_bits = 0ull;
+  hc.steps = 0;
+  hc.accepted = 0;
+  hc.max_steps = max_steps > 0 ? max_steps : 10000000ll;
+  hc.ycur = 0;
+  hc.done = ctx->time < t_end ? 0 : 1;
+  hc.status = 0;
+  hc.nonfinite = 0;
+  PHI_CK(cudaMemcpyAsync(ctx->ctl.ptr, &hc, sizeof(hc), cudaMemcpyHostToDevice, ctx->stream));
+  if (!ctx->rkf45_graph) {
+    PHI_CK(capture(ctx->stream, [&]() {
+      for (int i = 0; i < kGraphSteps; ++i) {
+        cudaError_t e = enqueue_rkf45_step(ctx, ctx->stream);
+        if (e != cudaSuccess) return e;
+      }
+      return cudaSuccess;
+    }, &ctx->rkf45_graph));
+  }
+  phi::Rkf45Ctl *hpin = nullptr;
+  PHI_CK(cudaMallocHost(&hpin, sizeof(phi::Rkf45Ctl)));
+  int result = PHI_OK;
+  // Two graphs in flight: the done flag of launch j is read while launch j+1
+  // runs; steps after completion are no-ops on the device.
+  PHI_CK(cudaGraphLaunch(ctx->rkf45_graph, ctx->stream));
+  for (;;) {
+    cudaError_t e = cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hpin, ctx->ctl.ptr, sizeof(phi::Rkf45Ctl), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      result = cuda_err(ctx, e, "rkf45 graph");
+      break;
+    }
+    if (hpin->done) break;
+  }
+  if (result == PHI_OK) {
+    hc = *hpin;
+    if (hc.ycur == 1) std::swap(ctx->y, ctx->y_alt);
+    ctx->time = hc.time;
+    if (stats) {
+      stats->steps = hc.steps;
+      stats->accepted = hc.accepted;
+      stats->final_time = hc.time;
+      stats->final_dt = hc.dt;
+      stats->max_error = hc.max_error;
+    }
+    if (hc.status == 1) {
+      ctx->error = "rkf45: step limit reached before t_end";
+      result = PHI_E_STEP_COLLAPSE;
+    } else if (hc.status == 2) {
+      ctx->error = "rkf45: non-finite error estimate";
+      result = PHI_E_NUMERIC;
+    }
+  }
+  cudaFreeHost(hpin);
+  // Captured graphs bake in the y / y_alt pointers; a swap invalidates them.
+  if (hc.ycur == 1) ctx->release_graphs();
+  return result;
+}

@@ -1,0 +1,236 @@
+"""Python binding of the HEOM integrator (tests, benchmarks, notebooks).
+
+`PhiParameters` mirrors the fields of PHI's `struct PhiParameters`
+(phi_parameters.h:32-122) that the propagation and steady-state paths read,
+with the same names and the same conventions:
+
+* `num_matsubara_terms` is K + 1, `hierarchy_truncation_level` is L + 1;
+* matrices are complex N x N numpy arrays (indexed [row, col]); they are
+  passed to the library column-major, as PHI stores them;
+* `bath_coupling_op` is (num_baths, N) for diagonal coupling
+  (`CorrelatedCouplingTerms`) or (num_baths, N, N) for `FullBathTerms`.
+
+`Hierarchy` owns one device context (one hierarchy instance on one GPU).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import capi
+
+HBAR = 5.3088354   # cm^-1 ps   (phi_parameters.h:13-14)
+K_B = 0.6950344    # cm^-1 / K  (phi_parameters.h:15-16)
+
+
+@dataclass
+class PhiParameters:
+    num_states: int = 0
+    time_indepenent_hamiltonian: Optional[np.ndarray] = None  # (sic), as in PHI
+    num_bath_couplings: int = 0
+    num_matsubara_terms: int = 1
+    hierarchy_truncation_level: int = 1
+    gamma: Optional[np.ndarray] = None
+    lambda_: Optional[np.ndarray] = None
+    bath_coupling_op: Optional[np.ndarray] = None
+    is_diagonal_bath_coupling: bool = False
+    is_full_bath_coupling: bool = False
+    bath_sites: Optional[np.ndarray] = None
+    initial_density_matrix: Optional[np.ndarray] = None
+    temperature: float = 300.0
+    hbar: float = HBAR
+    boltzmann_constant: float = K_B
+    is_rho_normalized: bool = True
+    timestep: float = 0.001
+    integration_time: float = 0.0
+    output_minimum_timestep: float = 0.01
+    rkf45_tolerance: float = 1e-6
+    rkf45_minimum_timestep: float = 1e-6
+    bicgstab_tolerance: float = 1e-6
+
+    @property
+    def bath_kind(self) -> int:
+        if self.is_full_bath_coupling:
+            return capi.PHI_BATH_FULL
+        if self.is_diagonal_bath_coupling:
+            return capi.PHI_BATH_DIAGONAL
+        return capi.PHI_BATH_INDEPENDENT
+
+    @property
+    def num_terms(self) -> int:
+        return self.num_bath_couplings * self.num_matsubara_terms
+
+    def fix_incompatible_combinations(self, method: str) -> None:
+        """RKF45 and the steady-state solver force normalised ADOs
+        (FixIncompatibleCombinations, phi_parameters.cc:817-829)."""
+        if method in ("rkf45", "bicgstab", "steady"):
+            self.is_rho_normalized = True
+
+
+def col_major(m: np.ndarray) -> np.ndarray:
+    """Complex N x N matrix -> interleaved column-major doubles."""
+    m = np.asarray(m, dtype=np.complex128)
+    return np.ascontiguousarray(m.T).view(np.float64).reshape(-1).copy()
+
+
+def from_col_major(buf: np.ndarray, n: int) -> np.ndarray:
+    """Interleaved column-major doubles -> complex N x N matrix."""
+    return np.asarray(buf, dtype=np.float64).view(np.complex128).reshape(n, n).T.copy()
+
+
+def state_to_matrices(state: np.ndarray, n: int) -> np.ndarray:
+    """Node-major hierarchy state (2*M*N*N doubles) -> (M, N, N) complex."""
+    s = np.asarray(state, dtype=np.float64).view(np.complex128).reshape(-1, n, n)
+    return np.transpose(s, (0, 2, 1)).copy()
+
+
+def matrices_to_state(mats: np.ndarray) -> np.ndarray:
+    m = np.asarray(mats, dtype=np.complex128)
+    return np.ascontiguousarray(np.transpose(m, (0, 2, 1))).view(np.float64).reshape(-1).copy()
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class Hierarchy:
+    """One hierarchy instance on one GPU (a phi_ctx)."""
+
+    def __init__(self, p: PhiParameters, precision: int = capi.PHI_PREC_FP64,
+                 device: int = 0, max_nodes: int = 0):
+        self.lib = capi.load()
+        n = int(p.num_states)
+        self.n = n
+        self._keep = []
+        d = capi.PhiProblemDesc()
+        d.num_states = n
+        d.num_baths = int(p.num_bath_couplings)
+        d.num_matsubara_terms = int(p.num_matsubara_terms)
+        d.truncation_level = int(p.hierarchy_truncation_level)
+        d.bath_kind = p.bath_kind
+        d.normalized = 1 if p.is_rho_normalized else 0
+        d.hbar = float(p.hbar)
+        d.boltzmann_constant = float(p.boltzmann_constant)
+        d.temperature = float(p.temperature)
+
+        def keep(a, dtype=np.float64):
+            a = np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1))
+            self._keep.append(a)
+            return a
+
+        d.hamiltonian = _dptr(keep(col_major(p.time_indepenent_hamiltonian)))
+        d.initial_density_matrix = _dptr(keep(col_major(p.initial_density_matrix)))
+        d.gamma = _dptr(keep(p.gamma))
+        d.lambda_ = _dptr(keep(p.lambda_))
+        if p.bath_coupling_op is not None and p.bath_kind != capi.PHI_BATH_INDEPENDENT:
+            v = np.asarray(p.bath_coupling_op, dtype=np.float64)
+            if p.bath_kind == capi.PHI_BATH_FULL:
+                # (nb, N, N) [row, col] -> per-bath column-major
+                v = np.ascontiguousarray(np.transpose(v.reshape(-1, n, n), (0, 2, 1)))
+            d.coupling = _dptr(keep(v))
+        if p.bath_sites is not None:
+            s = keep(p.bath_sites, np.int32)
+            d.bath_sites = s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        d.precision = precision
+        d.device = device
+        d.max_nodes = max_nodes
+        ctx = ctypes.c_void_p()
+        capi.check(self.lib.phi_gpu_create(ctypes.byref(d), ctypes.byref(ctx)))
+        self.ctx = ctx
+        M = ctypes.c_int64()
+        T = ctypes.c_int32()
+        N = ctypes.c_int32()
+        self._check(self.lib.phi_gpu_dims(self.ctx, ctypes.byref(M), ctypes.byref(T), ctypes.byref(N)))
+        self.num_nodes = M.value
+        self.num_terms = T.value
+
+    def _check(self, code):
+        capi.check(code, self.ctx)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.phi_gpu_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def state_len(self) -> int:
+        return 2 * self.num_nodes * self.n * self.n
+
+    def node_table(self):
+        MT = self.num_nodes * self.num_terms
+        mi = np.zeros(MT, np.int32)
+        nx = np.zeros(MT, np.int32)
+        pv = np.zeros(MT, np.int32)
+        self._check(self.lib.phi_gpu_get_node_table(self.ctx, mi.ctypes.data, nx.ctypes.data, pv.ctypes.data))
+        shape = (self.num_nodes, self.num_terms)
+        return mi.reshape(shape), nx.reshape(shape), pv.reshape(shape)
+
+    def get_state(self) -> np.ndarray:
+        out = np.zeros(self.state_len, np.float64)
+        self._check(self.lib.phi_gpu_get_state(self.ctx, out.ctypes.data))
+        return out
+
+    def set_state(self, state: np.ndarray) -> None:
+        s = np.ascontiguousarray(state, dtype=np.float64)
+        assert s.size == self.state_len
+        self._check(self.lib.phi_gpu_set_state(self.ctx, s.ctypes.data))
+
+    def rho0(self) -> np.ndarray:
+        out = np.zeros(2 * self.n * self.n, np.float64)
+        self._check(self.lib.phi_gpu_get_rho0(self.ctx, out.ctypes.data))
+        return from_col_major(out, self.n)
+
+    def apply(self, state: np.ndarray) -> np.ndarray:
+        s = np.ascontiguousarray(state, dtype=np.float64)
+        assert s.size == self.state_len
+        out = np.zeros_like(s)
+        self._check(self.lib.phi_gpu_apply(self.ctx, s.ctypes.data, out.ctypes.data))
+        return out
+
+    @property
+    def time(self) -> float:
+        t = ctypes.c_double()
+        self._check(self.lib.phi_gpu_get_time(self.ctx, ctypes.byref(t)))
+        return t.value
+
+    @time.setter
+    def time(self, v: float) -> None:
+        self._check(self.lib.phi_gpu_set_time(self.ctx, float(v)))
+
+    def rk4(self, dt: float, t_end: float, output_min_step: float = 0.0, capacity: int = 0):
+        """Returns (steps, times, rho_0 rows as (k, N, N) complex)."""
+        E2 = 2 * self.n * self.n
+        traj = np.zeros(max(capacity, 1) * E2, np.float64)
+        times = np.zeros(max(capacity, 1), np.float64)
+        ns = ctypes.c_int64()
+        no = ctypes.c_int64()
+        self._check(self.lib.phi_gpu_rk4(
+            self.ctx, float(dt), float(t_end), float(output_min_step),
+            traj.ctypes.data if capacity else None, times.ctypes.data if capacity else None,
+            int(capacity), ctypes.byref(ns), ctypes.byref(no)))
+        k = min(no.value, capacity)
+        rows = np.stack([from_col_major(traj[r * E2:(r + 1) * E2], self.n) for r in range(k)]) if k else \
+            np.zeros((0, self.n, self.n), np.complex128)
+        return ns.value, times[:k].copy(), rows
+
+    def rkf45(self, dt0: float, t_end: float, tol: float, min_dt: float, max_steps: int = 0):
+        st = capi.PhiRkf45Stats()
+        self._check(self.lib.phi_gpu_rkf45(self.ctx, float(dt0), float(t_end), float(tol),
+                                           float(min_dt), int(max_steps), ctypes.byref(st)))
+        return {"steps": st.steps, "accepted": st.accepted, "final_time": st.final_time,
+                "final_dt": st.final_dt, "max_error": st.max_error}
