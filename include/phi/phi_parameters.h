@@ -1,0 +1,121 @@
+// phi/phi_parameters.h -- drop-in PhiParameters for the B200 integrator.
+//
+// Same struct name, field names, units and conventions as PHI's
+// phi_parameters.h:32-122 for everything the propagation and steady-state
+// paths read, and the same parameter-file reader (ReadCommandLine /
+// ReadInputFile / FixIncompatibleCombinations, phi_parameters.cc:93-888):
+// `key=value` scalars, `Key:` matrix blocks read row by row into column-major
+// storage, MatsubaraTerms stored as K+1, HierarchyTruncation counting tier 0.
+// Inputs outside this library's scope (annealing Hamiltonians, Hilbert-space
+// truncation, time-local closure, filtering, restart input, spectra) are read
+// and then rejected by HierarchyIntegrator with a message.
+#ifndef PHI_B200_PHI_PARAMETERS_H_
+#define PHI_B200_PHI_PARAMETERS_H_
+
+#include <complex>
+#include <fstream>
+#include <string>
+
+#include "../phi_b200.h"
+
+typedef double Float;
+typedef std::complex<double> Complex;
+
+// Reduced Planck constant in [cm-1*ps] and Boltzmann constant in [cm-1/K]
+// (phi_parameters.h:13-16).
+#define HBAR 5.3088354
+#define K_B 0.6950344
+
+enum RunMethod {
+  BROKENINPUT,
+  NONE,
+  RK4,
+  RKF45,
+  RK4SPECTRUM,
+  RKF45SPECTRUM,
+  BICGSTABL,
+  BICGSTAB,
+  BICGSTABU,
+  PRINTHIERARCHY,
+  PRINTMEMORY
+};
+
+struct PHI_API PhiParameters {
+  int verbose;
+
+  Float hbar;
+  Float boltzmann_constant;
+
+  int num_states;
+  int hilbert_space_num_elements;
+  int hilbert_space_size;
+  int num_bath_couplings;
+  int num_matsubara_terms;  // K + 1
+
+  int hierarchy_truncation_level;  // L + 1
+  long long matrix_count;
+
+  Complex *time_indepenent_hamiltonian;
+  Complex *final_annealing_hamiltonian;
+  Complex *initial_annealing_hamiltonian;
+
+  Float temperature;
+
+  Float *gamma;
+  Float *lambda;
+  Float *bath_coupling_op;
+  int *multiple_independent_bath_indices;
+
+  Complex *initial_density_matrix;
+
+  Float integration_time;
+  Float timestep;
+  Float output_minimum_timestep;
+  Float start_time;
+  Float rkf45_minimum_timestep;
+  Float rkf45_tolerance;
+  Float bicgstab_tolerance;
+  Float filter_tolerance;
+
+  std::string output_filename;
+  std::string restart_input_filename;
+  std::string restart_output_filename;
+
+  bool is_truncated_system;
+  bool use_time_local_truncation;
+  bool is_multiple_independent_baths;
+  bool is_spectrum_calculation;
+  bool is_diagonal_bath_coupling;
+  bool is_full_bath_coupling;
+  bool is_rho_normalized;
+  bool is_restarted;
+  bool has_kappa;
+
+  int bicgstab_ell;
+  int num_threads;  // accepted for compatibility; the GPU path ignores it
+  bool are_parameters_valid;
+  RunMethod run_method;
+
+  // B200 additions: arithmetic of the Liouvillian (0 = FP64, 1 = mixed) and
+  // the CUDA device.
+  int precision;
+  int device;
+
+  PhiParameters();
+  ~PhiParameters();
+  PhiParameters(const PhiParameters &) = delete;
+  PhiParameters &operator=(const PhiParameters &) = delete;
+
+  void SetDefaults();
+  bool FileExists(const char *filename);
+  void FixIncompatibleCombinations();
+  void ReadCommandLine(int num_args, char *argv[]);
+  void ReadInputFile(std::string parameter_file);
+  void Write(std::ofstream *out, long long num_matrices);
+};
+
+// C(truncation - 1 + terms, terms): number of hierarchy nodes
+// (phi_parameters.cc:1138-1147).
+PHI_API long long GetHierarchyNodeCountEstimate(int truncation_level, int num_terms);
+
+#endif  // PHI_B200_PHI_PARAMETERS_H_

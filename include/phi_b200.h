@@ -27,6 +27,12 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#if defined(__GNUC__)
+#define PHI_API __attribute__((visibility("default")))
+#else
+#define PHI_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -103,20 +109,20 @@ typedef struct {
  * Launch(): Initialize, ConstructI, LinkHierarchyNodes, InitializePrefactors,
  * InitializeDensityMatrix (hierarchy_integrator.cc:49-62, :376-594,
  * :1038-1158, :1204-1466; hierarchy.cc:45-155). */
-int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out);
+PHI_API int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out);
 
 /* Same, from a PHI parameter file (PhiParameters::ReadInputFile and
  * FixIncompatibleCombinations, phi_parameters.cc:152-888).  method is one of
  * "rk4", "rkf45", "bicgstab" (decides the forced normalisation exactly as
  * FixIncompatibleCombinations does). */
-int phi_gpu_create_from_file(const char *path, const char *method, int32_t precision,
+PHI_API int phi_gpu_create_from_file(const char *path, const char *method, int32_t precision,
                              int32_t device, phi_ctx **out);
 
 /* Releases every device and host resource of the context. */
-int phi_gpu_destroy(phi_ctx *ctx);
+PHI_API int phi_gpu_destroy(phi_ctx *ctx);
 
 /* Hierarchy size: M nodes, T = num_baths * (K+1) terms, N states. */
-int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
+PHI_API int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
                  int32_t *num_states);
 
 /* Node table built on the device, copied to host buffers of M*T int32 each
@@ -124,26 +130,26 @@ int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
  * id of node i + e_t or -1; prev[i*T + t] = id of node i - e_t or -1.
  * Replaces the multi_index_map_ of ConstructI (hierarchy.cc:45-155) and the
  * neighbour lists of LinkHierarchyNodes (hierarchy_integrator.cc:1204-1338). */
-int phi_gpu_get_node_table(const phi_ctx *ctx, int32_t *multi_index, int32_t *next,
+PHI_API int phi_gpu_get_node_table(const phi_ctx *ctx, int32_t *multi_index, int32_t *next,
                            int32_t *prev);
 
 /* Whole-hierarchy state, host buffers of 2*M*N*N doubles. */
-int phi_gpu_set_state(phi_ctx *ctx, const double *state);
-int phi_gpu_get_state(const phi_ctx *ctx, double *state);
+PHI_API int phi_gpu_set_state(phi_ctx *ctx, const double *state);
+PHI_API int phi_gpu_get_state(const phi_ctx *ctx, double *state);
 
 /* rho_0 (node 0), host buffer of 2*N*N doubles.  Replaces density_matrix()
  * (hierarchy_integrator.cc:177-191), which returns the same storage order. */
-int phi_gpu_get_rho0(const phi_ctx *ctx, double *rho0);
+PHI_API int phi_gpu_get_rho0(const phi_ctx *ctx, double *rho0);
 
 /* One Liouvillian apply over every node: out = L(in), host buffers of
  * 2*M*N*N doubles.  Replaces a sweep of HierarchyUpdater::Get
  * (hierarchy_updater.h:36-52) over all nodes.  Input ADOs must be Hermitian
  * (PHI's formulation keeps every ADO Hermitian). */
-int phi_gpu_apply(phi_ctx *ctx, const double *in, double *out);
+PHI_API int phi_gpu_apply(phi_ctx *ctx, const double *in, double *out);
 
 /* Device-pointer variant: in/out are device buffers of M*N*N complex in the
  * context's precision; stream is a cudaStream_t (NULL = legacy default). */
-int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream);
+PHI_API int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream);
 
 /* Fixed-step RK4 from the current state (Rk4Integrate,
  * hierarchy_integrator.cc:2578-2939).  Steps while time < t_end with time
@@ -151,7 +157,7 @@ int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stre
  * (0-based) with i % ceil(output_min_step/dt) == 0, rho_0 is written to
  * traj[k*2*N*N] and its time to times[k] for k < capacity (either may be
  * NULL).  Returns the number of steps and of output rows. */
-int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min_step,
+PHI_API int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min_step,
                 double *traj, double *times, int64_t capacity, int64_t *num_steps,
                 int64_t *num_out);
 
@@ -160,16 +166,16 @@ int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min_step,
  * accept if error < tol or dt/2 < min_dt, grow x1.1 when error < tol/10,
  * shrink x0.5 on reject, last step clamped to t_end.  max_steps bounds the
  * attempted steps (0 = 10^7); hitting it returns PHI_E_STEP_COLLAPSE. */
-int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
+PHI_API int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
                   int64_t max_steps, phi_rkf45_stats *stats);
 
 /* Time carried by the context (advanced by the integrators). */
-int phi_gpu_get_time(const phi_ctx *ctx, double *time);
-int phi_gpu_set_time(phi_ctx *ctx, double time);
+PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);
+PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);
 
 /* Copies the text of the last error on this context (or of the last failed
  * create when ctx is NULL) into buf. */
-int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
+PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
 
 #ifdef __cplusplus
 }

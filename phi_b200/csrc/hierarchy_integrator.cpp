@@ -1,0 +1,252 @@
+// hierarchy_integrator.cpp -- drop-in HierarchyIntegrator facade over the C ABI
+// and PHI's output-file layout (hierarchy_integrator.cc:313-319 header,
+// :1148-1157 initial line, :2859-2880 RK4 rows, :2530-2558 / :2905-2924
+// closing lines).
+#include "../../include/phi/hierarchy_integrator.h"
+
+#include <cmath>
+#include <ctime>
+#include <fstream>
+#include <iomanip>
+#include <iostream>
+#include <vector>
+
+namespace phi {
+
+void set_create_error(const std::string &msg);
+
+int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std::string *err) {
+  auto reject = [&](const std::string &m) {
+    *err = m;
+    return PHI_E_INVALID;
+  };
+  if (!p.are_parameters_valid || p.run_method == BROKENINPUT) return reject("parameter error");
+  if (p.time_indepenent_hamiltonian == nullptr)
+    return reject("time-dependent (annealing) Hamiltonians are outside this library's scope");
+  if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
+    return reject("Hilbert-space truncation is outside this library's scope");
+  if (p.use_time_local_truncation) return reject("time-local truncation is outside this library's scope");
+  if (p.filter_tolerance > 0) return reject("adaptive hierarchy filtering is outside this library's scope");
+  if (p.is_restarted) return reject("restart input is outside this library's scope");
+  if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
+  if (p.initial_density_matrix == nullptr)
+    return reject("InitialDensityMatrix is required (the thermal guess needs LAPACK and is not supported)");
+  if (p.gamma == nullptr || p.lambda == nullptr) return reject("Gamma and Lambda are required");
+  *d = phi_problem_desc{};
+  d->num_states = p.num_states;
+  d->num_baths = p.num_bath_couplings;
+  d->num_matsubara_terms = p.num_matsubara_terms;
+  d->truncation_level = p.hierarchy_truncation_level;
+  d->bath_kind = p.is_full_bath_coupling ? PHI_BATH_FULL
+                 : p.is_diagonal_bath_coupling ? PHI_BATH_DIAGONAL : PHI_BATH_INDEPENDENT;
+  d->normalized = p.is_rho_normalized ? 1 : 0;
+  d->hbar = p.hbar;
+  d->boltzmann_constant = p.boltzmann_constant;
+  d->temperature = p.temperature;
+  d->hamiltonian = reinterpret_cast<const double *>(p.time_indepenent_hamiltonian);
+  d->initial_density_matrix = reinterpret_cast<const double *>(p.initial_density_matrix);
+  d->gamma = p.gamma;
+  d->lambda = p.lambda;
+  d->coupling = (p.is_full_bath_coupling || p.is_diagonal_bath_coupling) ? p.bath_coupling_op : nullptr;
+  d->bath_sites = (p.is_multiple_independent_baths && d->bath_kind == PHI_BATH_INDEPENDENT)
+                      ? p.multiple_independent_bath_indices : nullptr;
+  d->precision = p.precision;
+  d->device = p.device;
+  d->max_nodes = 0;
+  return PHI_OK;
+}
+
+}  // namespace phi
+
+HierarchyIntegrator::HierarchyIntegrator(PhiParameters *p) : parameters_(p) {}
+
+HierarchyIntegrator::~HierarchyIntegrator() {
+  if (ctx_) phi_gpu_destroy(ctx_);
+  delete[] result_;
+}
+
+void HierarchyIntegrator::Fail(int code, const std::string &msg) {
+  status_ = code;
+  error_ = msg;
+  if (parameters_->verbose > -2) std::cerr << "phi_b200: " << msg << "\n";
+}
+
+bool HierarchyIntegrator::Prepare() {
+  phi_problem_desc d;
+  std::string err;
+  int rc = phi::descriptor_from_parameters(*parameters_, &d, &err);
+  if (rc != PHI_OK) {
+    Fail(rc, err);
+    return false;
+  }
+  rc = phi_gpu_create(&d, &ctx_);
+  if (rc != PHI_OK) {
+    char buf[512];
+    phi_gpu_last_error(nullptr, buf, sizeof buf);
+    Fail(rc, buf);
+    return false;
+  }
+  phi_gpu_set_time(ctx_, parameters_->start_time);
+  return true;
+}
+
+void HierarchyIntegrator::Launch() {
+  if (!parameters_->are_parameters_valid || parameters_->run_method == BROKENINPUT ||
+      parameters_->run_method == NONE) {
+    if (!parameters_->are_parameters_valid) std::cout << "Parameter error.\n";
+    status_ = PHI_E_INVALID;
+    return;
+  }
+  Run(0, parameters_->num_threads, parameters_->run_method);
+  if (parameters_->verbose > -2) std::cout << "Done.\n";
+}
+
+void HierarchyIntegrator::Run(int, int, RunMethod method) {
+  if (method != RK4 && method != RKF45) {
+    Fail(PHI_E_INVALID, "run method not provided by this build of the library");
+    return;
+  }
+  if (!Prepare()) return;
+  const int N = parameters_->num_states;
+  int64_t M = 0;
+  phi_gpu_dims(ctx_, &M, nullptr, nullptr);
+  std::ofstream out;
+  if (!parameters_->output_filename.empty()) out.open(parameters_->output_filename.c_str());
+  // PrepareForOutput (hierarchy_integrator.cc:313-319) and the t = start line
+  // of InitializeDensityMatrix (:1148-1157).
+  if (out.is_open()) {
+    parameters_->Write(&out, M);
+    out << "#Total Number of matrices:" << M << std::endl;
+    out << "#Threads=" << parameters_->num_threads << "\n";
+    out << "#Integrator=" << (method == RK4 ? "rk4" : "rkf45") << "\n";
+    out << "#-------------\n";
+    out << parameters_->start_time << " ";
+    for (int i = 0; i < N * N; ++i) out << parameters_->initial_density_matrix[i] << " ";
+    out << "\n" << std::flush;
+  }
+  if (method == RK4) RunRk4(out);
+  else RunRkf45(out);
+  if (status_ == PHI_OK) {
+    delete[] result_;
+    result_ = new Complex[(size_t)N * N];
+    phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(result_));
+    has_result_ = true;
+  }
+}
+
+void HierarchyIntegrator::RunRk4(std::ofstream &out) {
+  const PhiParameters &p = *parameters_;
+  const int N = p.num_states;
+  const double dt = p.timestep;
+  // Rows written after steps i with i % ceil(OutputMinimumTimestep/dt) == 0
+  // (hierarchy_integrator.cc:2617-2618, :2858-2880).
+  const long long of = (long long)std::ceil(p.output_minimum_timestep / dt);
+  long long rows = 0;
+  {
+    double t = p.start_time;
+    long long i = 0;
+    while (t < p.integration_time) {
+      t += dt;
+      if (of > 0 && i % of == 0) ++rows;
+      ++i;
+    }
+  }
+  std::vector<double> traj((size_t)std::max<long long>(rows, 1) * 2 * N * N);
+  std::vector<double> times((size_t)std::max<long long>(rows, 1));
+  int64_t nsteps = 0, nout = 0;
+  const std::time_t t1 = std::time(nullptr);
+  int rc = phi_gpu_rk4(ctx_, dt, p.integration_time, p.output_minimum_timestep, traj.data(),
+                       times.data(), rows, &nsteps, &nout);
+  const std::time_t t2 = std::time(nullptr);
+  if (rc != PHI_OK) {
+    char buf[512];
+    phi_gpu_last_error(ctx_, buf, sizeof buf);
+    Fail(rc, buf);
+    return;
+  }
+  steps_ = nsteps;
+  accepted_ = nsteps;
+  if (!out.is_open()) return;
+  const Complex *rows_c = reinterpret_cast<const Complex *>(traj.data());
+  for (long long r = 0; r < std::min<long long>(nout, rows); ++r) {
+    out << times[r];
+    for (int j = 0; j < N * N; ++j) out << " " << rows_c[r * N * N + j];
+    out << "\n";
+  }
+  std::vector<Complex> rho((size_t)N * N);
+  phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(rho.data()));
+  double tnow = 0;
+  phi_gpu_get_time(ctx_, &tnow);
+  if (p.verbose > -1) {
+    out << "#Total number of integration steps = " << nsteps << "\n"
+        << "#Total integration time = " << std::difftime(t2, t1) / 60 << " mins\n";
+  }
+  out << std::setw(20) << std::setprecision(6) << tnow << std::setw(6) << std::setprecision(4);
+  for (int j = 0; j < N * N; ++j) out << " " << rho[j];
+  out << "\n";
+}
+
+void HierarchyIntegrator::RunRkf45(std::ofstream &out) {
+  const PhiParameters &p = *parameters_;
+  const int N = p.num_states;
+  phi_rkf45_stats st{};
+  const std::time_t t1 = std::time(nullptr);
+  int rc = phi_gpu_rkf45(ctx_, p.timestep, p.integration_time, p.rkf45_tolerance,
+                         p.rkf45_minimum_timestep, 0, &st);
+  const std::time_t t2 = std::time(nullptr);
+  if (rc != PHI_OK) {
+    char buf[512];
+    phi_gpu_last_error(ctx_, buf, sizeof buf);
+    Fail(rc, buf);
+    return;
+  }
+  steps_ = st.steps;
+  accepted_ = st.accepted;
+  if (!out.is_open()) return;
+  std::vector<Complex> rho((size_t)N * N);
+  phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(rho.data()));
+  if (p.verbose > -1) {
+    out << "#Total number of integration steps = " << st.steps << "\n"
+        << "#Total number of accepted integration steps = " << st.accepted << "\n"
+        << "#Total integration time = " << std::difftime(t2, t1) / 60 << " mins.\n";
+  }
+  out << std::setw(20) << std::setprecision(6) << st.final_time << std::setw(6)
+      << std::setprecision(4);
+  for (int j = 0; j < N * N; ++j) out << " " << rho[j];
+  out << std::endl;
+}
+
+Complex *HierarchyIntegrator::density_matrix() {
+  const int N = parameters_->num_states;
+  Complex *rho = new Complex[(size_t)N * N];
+  const Complex *src = has_result_ ? result_ : parameters_->initial_density_matrix;
+  for (int i = 0; i < N * N; ++i) rho[i] = src ? src[i] : Complex(0, 0);
+  return rho;
+}
+
+extern "C" int phi_gpu_create_from_file(const char *path, const char *method, int32_t precision,
+                                        int32_t device, phi_ctx **out) {
+  if (!out || !path || !method) return PHI_E_INVALID;
+  *out = nullptr;
+  char prog[] = "phi_b200";
+  std::string ps(path), ms(method);
+  std::vector<char> a1(ps.begin(), ps.end()), a2(ms.begin(), ms.end());
+  a1.push_back(0);
+  a2.push_back(0);
+  char *argv[3] = {prog, a1.data(), a2.data()};
+  PhiParameters p;
+  p.verbose = -2;
+  std::streambuf *old = std::cout.rdbuf(nullptr);  // the reader echoes to stdout
+  p.ReadCommandLine(3, argv);
+  std::cout.rdbuf(old);
+  p.precision = precision;
+  p.device = device;
+  phi_problem_desc d;
+  std::string err;
+  int rc = phi::descriptor_from_parameters(p, &d, &err);
+  if (rc != PHI_OK) {
+    phi::set_create_error(err);  // reported by phi_gpu_last_error(NULL, ...)
+    return rc;
+  }
+  return phi_gpu_create(&d, out);
+}

@@ -217,6 +217,8 @@ int setup_constants(phi_ctx *ctx) {
   return PHI_OK;
 }
 
+void set_create_error(const std::string &msg) { g_create_error = msg; }
+
 }  // namespace phi
 
 // --------------------------------------------------------------------------
@@ -247,6 +249,16 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   for (int k = 0; k < 2 * N * N; ++k)
     if (!std::isfinite(d.hamiltonian[k]) || !std::isfinite(d.initial_density_matrix[k]))
       return fail(nullptr, PHI_E_INVALID, "non-finite value in the Hamiltonian or initial density matrix");
+  if (d.truncation_level > 1 && (d.normalized || d.bath_kind == PHI_BATH_DIAGONAL)) {
+    // The normalised prefactors divide by sqrt(n |c_t|) (hierarchy_integrator.cc
+    // :1430-1436); c_t vanishes when gamma <= 0 or lambda == 0 (:441-469).
+    for (int b = 0; b < d.num_baths; ++b)
+      if (!(d.gamma[b] > 0) || d.lambda[b] == 0 || !std::isfinite(d.gamma[b]) || !std::isfinite(d.lambda[b]))
+        if (d.normalized && d.bath_kind != PHI_BATH_DIAGONAL)
+          return fail(nullptr, PHI_E_INVALID,
+                      "bath " + std::to_string(b) + ": gamma must be > 0 and lambda non-zero for a "
+                      "normalised hierarchy");
+  }
   if (!is_hermitian(d.initial_density_matrix, N, nullptr))
     return fail(nullptr, PHI_E_INVALID,
                 "initial density matrix is not Hermitian (PHI's hierarchy keeps every ADO Hermitian)");

@@ -1,0 +1,130 @@
+"""Problem builders shared by the tests.
+
+`reference_fixture_case(name)` restates the problems of the reference's own
+golden tests (src/hierarchy_integrator_test.cc): the fixture of :27-44 (hbar =
+k_B = 1, T = 2, run to t = 1), the two-state Hamiltonian of :46-54, the weak
+bath of :143-151 (gamma = 1, lambda = 0.01 for every term: the reference's
+`1.0 + i/10` is integer division), the coupling operators of :163-229 and
+rho(0) = |0><0| (:231-239).  Only the cases in scope for this path are listed
+(static Hamiltonian, untruncated Hilbert space, no time-local closure).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from phi_b200.heom import PhiParameters
+
+# name -> (golden vector key, builder kwargs)
+REFERENCE_CASES = {
+    "TestVacuum": ("kVacuumSoln", dict(baths=1, truncation=1)),
+    "TestWeakIndependentBath": ("kWeakIndependentCouplingSoln", dict(baths=2, truncation=2)),
+    "TestWeakIndependentDiagonalBath": ("kWeakIndependentCouplingSoln",
+                                        dict(baths=2, truncation=2, coupling="diag_identity")),
+    "WeakIndependentFullBath": ("kWeakIndependentCouplingSoln",
+                                dict(baths=2, truncation=2, coupling="full_identity")),
+    "TestWeakDiagonalBath": ("kWeakDiagonalCouplingSoln",
+                             dict(baths=2, truncation=2, coupling="diag_alternating")),
+    "TestWeakFullDiagonalBath": ("kWeakDiagonalCouplingSoln",
+                                 dict(baths=2, truncation=2, coupling="full_diag_alternating")),
+    "TestWeakFullBath": ("kWeakFullCouplingSoln",
+                         dict(baths=2, truncation=2, coupling="full_alternating")),
+    "TestWeakIndependentBathMatsubara": ("kWeakIndependentCouplingMatsubaraSoln",
+                                         dict(baths=2, truncation=3, matsubara=3, temperature=0.5)),
+    "TestWeakDiagonalBathMatsubara": ("kWeakIndependentCouplingMatsubaraSoln",
+                                      dict(baths=2, truncation=3, matsubara=3, temperature=0.5,
+                                           coupling="diag_identity")),
+    "TestWeakFullBathMatsubara": ("kWeakIndependentCouplingMatsubaraSoln",
+                                  dict(baths=2, truncation=3, matsubara=3, temperature=0.5,
+                                       coupling="full_identity")),
+}
+
+# Tolerances of the reference's assertions (hierarchy_integrator_test.cc:316-340).
+RK4_TOL = 1e-6
+RKF45_TOL = 1e-3
+
+
+def reference_fixture_case(name: str) -> PhiParameters:
+    _, kw = REFERENCE_CASES[name]
+    n = 2
+    nb = kw["baths"]
+    p = PhiParameters(
+        num_states=n,
+        time_indepenent_hamiltonian=np.array([[0.5, 0.5], [0.5, -0.5]], np.complex128),
+        num_bath_couplings=nb, num_matsubara_terms=kw.get("matsubara", 1),
+        hierarchy_truncation_level=kw["truncation"],
+        gamma=np.full(nb, 1.0), lambda_=np.full(nb, 0.01),
+        temperature=kw.get("temperature", 2.0), hbar=1.0, boltzmann_constant=1.0,
+        integration_time=1.0, timestep=0.001, rkf45_tolerance=1e-6, rkf45_minimum_timestep=1e-6)
+    rho = np.zeros((n, n), np.complex128)
+    rho[0, 0] = 1.0
+    p.initial_density_matrix = rho
+    c = kw.get("coupling")
+    if c == "diag_identity":
+        p.bath_coupling_op = np.eye(n)[:nb]
+        p.is_diagonal_bath_coupling = True
+    elif c == "full_identity":
+        V = np.zeros((nb, n, n))
+        for i in range(nb):
+            V[i, i, i] = 1.0
+        p.bath_coupling_op = V
+        p.is_full_bath_coupling = True
+    elif c == "diag_alternating":
+        p.bath_coupling_op = np.array([[(-1.0) ** (i + j) for j in range(n)] for i in range(nb)])
+        p.is_diagonal_bath_coupling = True
+    elif c == "full_diag_alternating":
+        V = np.zeros((nb, n, n))
+        for i in range(nb):
+            for j in range(n):
+                V[i, j, j] = (-1.0) ** (i + j)
+        p.bath_coupling_op = V
+        p.is_full_bath_coupling = True
+    elif c == "full_alternating":
+        V = np.array([[[(-1.0) ** (i + j + k) for k in range(n)] for j in range(n)]
+                      for i in range(nb)])
+        p.bath_coupling_op = V
+        p.is_full_bath_coupling = True
+    return p
+
+
+def random_problem(kind: str = "independent", n: int = 3, matsubara: int = 2, truncation: int = 3,
+                   baths: int | None = None, seed: int = 0, normalized: bool = True,
+                   complex_h: bool = False, scale: float = 50.0) -> PhiParameters:
+    """Seeded random problem in PHI's units (cm^-1, ps, K)."""
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(n, n)) + (1j * rng.normal(size=(n, n)) if complex_h else 0)
+    H = (A + np.conj(A).T) / 2 * scale
+    p = PhiParameters(num_states=n, time_indepenent_hamiltonian=np.asarray(H, np.complex128),
+                      num_matsubara_terms=matsubara, hierarchy_truncation_level=truncation,
+                      temperature=300.0, is_rho_normalized=normalized)
+    rho = np.zeros((n, n), np.complex128)
+    rho[0, 0] = 0.7
+    rho[n - 1, n - 1] += 0.3
+    if n > 1:
+        rho[0, n - 1] = 0.1 + 0.05j
+        rho[n - 1, 0] = 0.1 - 0.05j
+    p.initial_density_matrix = rho
+    if kind == "independent":
+        nb = n
+    elif kind == "diagonal":
+        nb = baths or 2
+        p.is_diagonal_bath_coupling = True
+        p.bath_coupling_op = rng.normal(size=(nb, n))
+    elif kind == "full":
+        nb = baths or 2
+        p.is_full_bath_coupling = True
+        V = rng.normal(size=(nb, n, n))
+        p.bath_coupling_op = (V + V.transpose(0, 2, 1)) / 2
+    else:
+        raise ValueError(kind)
+    p.num_bath_couplings = nb
+    p.gamma = rng.uniform(5.0, 20.0, size=nb)
+    p.lambda_ = rng.uniform(10.0, 40.0, size=nb)
+    return p
+
+
+def random_hermitian_state(M: int, n: int, seed: int = 1) -> np.ndarray:
+    """(M, N, N) random Hermitian ADOs, node-major interleaved doubles."""
+    rng = np.random.default_rng(seed)
+    A = rng.normal(size=(M, n, n)) + 1j * rng.normal(size=(M, n, n))
+    A = (A + np.conj(np.transpose(A, (0, 2, 1)))) / 2
+    return np.ascontiguousarray(np.transpose(A, (0, 2, 1))).view(np.float64).reshape(-1).copy()

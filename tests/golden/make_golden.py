@@ -1,0 +1,123 @@
+"""Generates the golden fixtures under tests/golden/ from the reference.
+
+Run in a container that has the reference tree and the reference build
+(oracle/_ref/ref_driver, from `make -C oracle`):
+
+    python tests/golden/make_golden.py /root/reference
+
+Outputs (committed; the GPU host has no reference tree):
+  reference_tests.json  rho_0 vectors hard-coded in the reference's own tests
+                        (src/hierarchy_integrator_test.cc), read as text
+  ref_outputs.json      rho_0 printed with %.17g by the reference build for
+                        the problems listed in CASES (builder + arguments)
+  ref_order.json        node order of the reference's ConstructI for a set of
+                        (terms, truncation) pairs
+"""
+from __future__ import annotations
+
+import json
+import os
+import re
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.dirname(HERE))
+
+from oracle import oracle as O  # noqa: E402
+from phi_b200 import configs  # noqa: E402
+import cases  # noqa: E402
+
+# (case id, builder, builder kwargs, method, run kwargs)
+CASES = []
+for name in cases.REFERENCE_CASES:
+    for method in ("rk4", "rkf45"):
+        CASES.append((f"{name}/{method}", "reference_fixture_case", {"name": name}, method, {}))
+for kind in ("independent", "diagonal", "full"):
+    for method in ("rk4", "rkf45"):
+        for seed, (n, K1, tr) in enumerate([(3, 2, 3), (4, 1, 4), (2, 3, 3)]):
+            CASES.append((f"random_{kind}_{n}_{K1}_{tr}/{method}", "random_problem",
+                          {"kind": kind, "n": n, "matsubara": K1, "truncation": tr, "seed": seed,
+                           "complex_h": seed == 1},
+                          method, {"timestep": 0.001, "t_end": 0.05}))
+CASES.append(("random_independent_unnormalized/rk4", "random_problem",
+              {"kind": "independent", "n": 3, "matsubara": 2, "truncation": 3, "seed": 5,
+               "normalized": False}, "rk4", {"timestep": 0.001, "t_end": 0.05}))
+CASES.append(("spin_boson_L10/rk4", "config:spin_boson", {}, "rk4",
+              {"timestep": 0.001, "t_end": 2.0}))
+CASES.append(("spin_boson_L10_short/rkf45", "config:spin_boson", {}, "rkf45",
+              {"timestep": 0.001, "t_end": 0.2}))
+CASES.append(("frenkel7_L3/rkf45", "config:frenkel7", {"depth": 3}, "rkf45",
+              {"timestep": 0.001, "t_end": 0.05}))
+CASES.append(("frenkel7_L3/rk4", "config:frenkel7", {"depth": 3}, "rk4",
+              {"timestep": 0.001, "t_end": 0.05}))
+CASES.append(("chain4_L4/rk4", "config:chain4", {"depth": 4}, "rk4",
+              {"timestep": 0.001, "t_end": 0.05}))
+CASES.append(("ring24_L2/rk4", "config:ring24", {"depth": 2}, "rk4",
+              {"timestep": 0.001, "t_end": 0.01}))
+
+ORDERS = [(1, 5), (2, 4), (3, 5), (5, 4), (7, 3), (6, 5), (12, 3), (14, 4), (24, 3)]
+
+
+def build(builder: str, kw: dict):
+    if builder.startswith("config:"):
+        return getattr(configs, builder.split(":", 1)[1])(**kw)
+    return getattr(cases, builder)(**kw)
+
+
+def parse_reference_tests(ref_root: str) -> dict:
+    text = open(os.path.join(ref_root, "src", "hierarchy_integrator_test.cc")).read()
+    keys = {k for k, _ in cases.REFERENCE_CASES.values()}
+    out = {}
+    for key in sorted(keys):
+        m = re.search(r"const Complex %s\[\] = \{(.*?)\};" % key, text, re.S)
+        vals = []
+        for c in re.findall(r"Complex\(([^)]*)\)", m.group(1)):
+            parts = [float(x) for x in c.split(",")]
+            vals.append([parts[0], parts[1] if len(parts) > 1 else 0.0])
+        out[key] = vals  # storage (column-major) order, as the test lists them
+    return out
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if not O.ref_available():
+        raise SystemExit("build the reference first: make -C oracle")
+    golden = parse_reference_tests(ref_root)
+    with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
+        json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)
+
+    outs = []
+    for cid, builder, kw, method, run in CASES:
+        p = build(builder, kw)
+        try:
+            rho, secs = O.run_reference(p, method, 1, timeout=60, **run)
+        except subprocess.TimeoutExpired:
+            # The reference's RKF45 accept test races with its writer thread
+            # (hierarchy_integrator.cc:2355 vs :2434-2437) and can deadlock.
+            outs.append({"id": cid, "builder": builder, "kwargs": kw, "method": method,
+                         "run": run, "unavailable": "reference run timed out (RKF45 thread race)"})
+            print(f"{cid}: TIMEOUT", flush=True)
+            continue
+        outs.append({"id": cid, "builder": builder, "kwargs": kw, "method": method, "run": run,
+                     "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]})
+        print(f"{cid}: {secs:.3f}s", flush=True)
+    with open(os.path.join(HERE, "ref_outputs.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
+
+    orders = []
+    for T, tr in ORDERS:
+        p = cases.random_problem("independent", n=T, matsubara=1, truncation=tr, seed=0)
+        mi = O.reference_order(p)
+        orders.append({"terms": T, "truncation": tr, "multi_index": mi.tolist()})
+        print(f"order T={T} trunc={tr}: {mi.shape[0]} nodes", flush=True)
+    with open(os.path.join(HERE, "ref_order.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "orders": orders}, f)
+
+
+if __name__ == "__main__":
+    main()
