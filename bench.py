@@ -1,0 +1,347 @@
+"""Benchmark: hierarchy-node Liouvillian applies per second of the RKF45
+propagation of the 7-site Frenkel exciton hierarchy (N = 7, 7 Drude baths,
+K = 1, depth L = 6: 38,760 nodes of 7x7 complex128; RKF45 tol 1e-6 to 1 ps).
+
+One bench "step" is one attempted RKF45 step over the whole hierarchy: six
+fused Liouvillian-apply + stage-combine kernels over all 38,760 nodes, the
+error max-reduction and the device-side accept/step-size control.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phi_b200|reference]
+                    [--precision fp64|mixed]
+
+With N > 1 (torchrun, one rank per GPU) every rank integrates its own replica
+of the hierarchy (the path has no exchange step): weak scaling, value = all
+ranks' applies / max-over-ranks device time.  `--impl reference` times the
+reference PHI build (oracle/_ref) on this host's cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "hierarchy-node applies/sec and RKF45 steps/sec at rho_0 err<=1e-6 vs FP64 GPU"
+UNIT = "node-applies/s"
+T_END = 1.0
+DT0 = 0.001
+TOL = 1e-6
+MIN_DT = 1e-6
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--warmup", type=int, default=16)
+    ap.add_argument("--impl", default="phi_b200", choices=["phi_b200", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from phi_b200 import configs
+    p = configs.frenkel7()
+    p.fix_incompatible_combinations("rkf45")
+    return p
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_port(p, seconds_budget=12.0):
+    """The oracle (C restatement, one core) on a bounded sample: Liouvillian
+    applies over the full hierarchy until ~seconds_budget of CPU work."""
+    import numpy as np
+    from oracle import oracle as O
+    o = O.Oracle(p)
+    s = o.initial_state()
+    rng = np.random.default_rng(0)
+    s = s + 1e-3 * rng.normal(size=s.size)
+    n_apply = 0
+    t0 = time.perf_counter()
+    while True:
+        o.apply(s)
+        n_apply += 1
+        if time.perf_counter() - t0 > seconds_budget / 2 or n_apply >= 16:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n_apply * o.M / dt, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n_apply} Liouvillian applies over the {o.M}-node hierarchy "
+                      f"({dt:.1f} s, single-thread C restatement)"}
+
+
+def run_reference_arm(args):
+    """Times the reference PHI build (oracle/_ref/ref_driver) with all host
+    threads: per-step time from two runs of different length (its setup is
+    O(M^2) and is excluded by the difference)."""
+    from oracle import oracle as O
+    p = workload()
+    threads = os.cpu_count() or 1
+    res = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+           "config": {"workload": "frenkel7_K1_L6 (N=7, 7 Drude baths, 38760 nodes), RKF45 tol 1e-6",
+                      "seed": p.seed, "threads": threads}}
+    if not O.ref_available():
+        res["unavailable"] = "reference build oracle/_ref/ref_driver not present"
+        return res
+    runs = []
+    try:
+        for t_end in (0.002, 0.002 + 0.001 * max(2, min(args.steps, 8))):
+            with tempfile.TemporaryDirectory() as d:
+                out = os.path.join(d, "phi.out")
+                prm = os.path.join(d, "in.prm")
+                rho_f = os.path.join(d, "rho.txt")
+                with open(prm, "w") as f:
+                    f.write(O.param_file_text(p, timestep=DT0, t_end=t_end, output_file=out)
+                            .replace("verbose=-2", "verbose=0"))
+                t0 = time.perf_counter()
+                subprocess.run([O.REF_DRIVER, "run", prm, "rkf45", str(threads), rho_f], check=True,
+                               timeout=900, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+                wall = time.perf_counter() - t0
+                steps = None
+                for ln in open(out):
+                    if ln.startswith("#Total number of integration steps"):
+                        steps = int(ln.split("=")[1])
+                runs.append((wall, steps))
+    except subprocess.TimeoutExpired:
+        res["unavailable"] = "reference RKF45 run timed out (its accept test races with the writer thread)"
+        return res
+    (wa, sa), (wb, sb) = runs
+    if sa is None or sb is None or sb <= sa or wb <= wa:
+        res["unavailable"] = f"could not difference the reference runs: {runs}"
+        return res
+    M = 38760
+    per_step = (wb - wa) / (sb - sa)
+    value = 6 * M / per_step
+    res.update({"value": value, "ms_per_step": per_step * 1e3,
+                "rkf45_steps_per_s": 1.0 / per_step,
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "sample": f"RKF45 steps {sa} and {sb} (t_end differenced), "
+                                           f"{threads} threads"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+    return res
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference_arm(args)), flush=True)
+        return
+
+    import torch
+    import numpy as np
+    from phi_b200 import capi
+    from phi_b200.heom import Hierarchy
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    prec = capi.PHI_PREC_MIXED if args.precision == "mixed" else capi.PHI_PREC_FP64
+    p = workload()
+    N = p.num_states
+
+    # ---- device-resident throughput (value) ----
+    h = Hierarchy(p, precision=prec, device=local_rank)
+    M = h.num_nodes
+    stream = torch.cuda.ExternalStream(h.stream_handle(), device=local_rank)
+    h.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    st = h.rkf45_advance(-1.0, T_END, TOL, MIN_DT, args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    steps_done = int(st["steps"])
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+        sd = torch.tensor([steps_done], device="cuda")
+        dist.all_reduce(sd, op=dist.ReduceOp.SUM)
+        total_steps = int(sd.item())
+    else:
+        total_steps = steps_done
+    applies = 6 * M * total_steps
+    value = applies / (t_max / 1e3)
+    ms_per_step = t_max / max(steps_done, 1)
+
+    # ---- dominant kernel in isolation: one apply launch over all nodes ----
+    E = N * N
+    x = torch.randn(M * E * 2, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    reps = 20
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            capi.check(h.lib.phi_gpu_apply_device(h.ctx, x.data_ptr(), y.data_ptr(), stream.cuda_stream), h.ctx)
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ea.record(stream)
+    for _ in range(reps):
+        capi.check(h.lib.phi_gpu_apply_device(h.ctx, x.data_ptr(), y.data_ptr(), stream.cuda_stream), h.ctx)
+    eb.record(stream)
+    eb.synchronize()
+    apply_ms = ea.elapsed_time(eb) / reps
+    h.close()
+
+    # ---- end to end through the C ABI with host buffers ----
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    h2 = Hierarchy(p, precision=prec, device=local_rank)
+    st2 = h2.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup + args.steps)
+    rho0 = h2.rho0()
+    h2.close()
+    e2e_s = time.perf_counter() - t0
+    e2e_steps = int(st2["steps"])
+    e2e_value = 6 * M * e2e_steps / e2e_s
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = 6 * M * e2e_steps * world / float(t.item())
+    h2d = (2 * E + 2 * E + 2 * 7) * 8  # H, rho(0), gamma, lambda
+    d2h = 2 * E * 8 + ((e2e_steps + 15) // 16 + 1) * 320  # rho_0 + control-block polls
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        S = M * E * 16
+        step_bytes = 36 * S           # fused RKF45 step
+        achieved = step_bytes / (ms_per_step / 1e3) / 1e9
+        apply_bytes = 2 * S
+        apply_gbs = apply_bytes / (apply_ms / 1e3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                traffic = json.load(open(tpath)).get("rkf45_step_dram_bytes")
+            except Exception:
+                traffic = None
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128" if prec == capi.PHI_PREC_FP64 else "c64+c128",
+            "data": "synthetic (seeded frenkel7, numpy default_rng seed 7)",
+            "config": {"workload": "frenkel7_K1_L6: 7-site Frenkel exciton, 7 Drude baths, K=1, L=6, "
+                                   "38760 nodes of 7x7, RKF45 tol 1e-6 to 1 ps",
+                       "nodes": M, "num_states": N, "terms": h.num_terms if False else 14,
+                       "precision": args.precision, "parallelism": f"replicas x{world}",
+                       "l2": "working set 9 x 30.4 MB state buffers = 274 MB > 126 MB L2"},
+            "rkf45_steps_per_s": total_steps / (t_max / 1e3),
+            "steps_timed": steps_done,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "heom_stage_kernel x6 + rkf45_control (one RKF45 step)",
+                         "algorithmic_bytes_per_step": step_bytes, "peak_kind": peak_kind},
+            "apply_kernel": {"ms": apply_ms, "algorithmic_bytes": apply_bytes, "achieved_gbs": apply_gbs,
+                             "frac": apply_gbs / peak, "node_applies_per_s": M / (apply_ms / 1e3)},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / max(e2e_steps, 1),
+                    "d2h_bytes_per_step": d2h / max(e2e_steps, 1),
+                    "what": "create (hierarchy built on device) + RKF45 + rho_0 read-back + destroy, "
+                            "host wall clock through the C ABI", "rho0_trace": float(np.trace(rho0).real)},
+            "gpu_launches": ((steps_done + 15) // 16) * 16 * 7,
+            "clocks": clocks,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline_port(p)
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

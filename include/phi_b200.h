@@ -169,6 +169,18 @@ PHI_API int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_min
 PHI_API int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
                   int64_t max_steps, phi_rkf45_stats *stats);
 
+/* Advances the adaptive integrator by exactly `steps` attempted RKF45 steps
+ * (fewer if t_end is reached first), with the same step control as
+ * phi_gpu_rkf45.  dt0 > 0 starts a new run; dt0 <= 0 continues the step size
+ * and tableau scaling of the previous call.  Reaching the step count is not
+ * an error. */
+PHI_API int phi_gpu_rkf45_advance(phi_ctx *ctx, double dt0, double t_end, double tol,
+                                  double min_dt, int64_t steps, phi_rkf45_stats *stats);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or timing events after the library's. */
+PHI_API int phi_gpu_stream(const phi_ctx *ctx, void **stream);
+
 /* Time carried by the context (advanced by the integrators). */
 PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);
 PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);

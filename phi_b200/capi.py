@@ -97,6 +97,9 @@ SIGNATURES = [
                             POINTER(c_int64), POINTER(c_int64)]),
     ("phi_gpu_rkf45", c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int64,
                               POINTER(PhiRkf45Stats)]),
+    ("phi_gpu_rkf45_advance", c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int64,
+                                      POINTER(PhiRkf45Stats)]),
+    ("phi_gpu_stream", c_int, [c_void_p, POINTER(c_void_p)]),
     ("phi_gpu_get_time", c_int, [c_void_p, POINTER(c_double)]),
     ("phi_gpu_set_time", c_int, [c_void_p, c_double]),
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),

@@ -130,9 +130,10 @@ __global__ void scan_block_sums_kernel(long long *block_sums, long long nblocks,
 
 // Scatter the kept candidates into tier order.
 __global__ void scatter_tier_kernel(uint8_t *mi, int T, long long prev_first, long long C,
-                                    long long num_cand, long long tier_first, Binom binom,
-                                    const uint8_t *keep, const long long *block_offsets,
-                                    int32_t *rank_to_id) {
+                                    long long num_cand, long long tier_first, long long tier_count,
+                                    Binom binom, const uint8_t *keep,
+                                    const long long *block_offsets, int32_t *rank_to_id,
+                                    int *bad) {
   __shared__ int warp_prefix[kScanBlock / 32];
   long long q = blockIdx.x * (long long)kScanBlock + threadIdx.x;
   int flag = q < num_cand ? keep[q] : 0;
@@ -155,6 +156,10 @@ __global__ void scatter_tier_kernel(uint8_t *mi, int T, long long prev_first, lo
     long long id = tier_first + pos;
     int t;
     unsigned long long r = candidate_rank(mi, T, prev_first, C, q, binom, &t);
+    if (pos < 0 || pos >= tier_count || r >= (unsigned long long)tier_count) {
+      atomicExch(bad, 1);  // never write outside the tier
+      return;
+    }
     const long long k = q / C;
     const long long n = q - k * C;
     const uint8_t *src = mi + (prev_first + n) * T;
@@ -167,7 +172,7 @@ __global__ void scatter_tier_kernel(uint8_t *mi, int T, long long prev_first, lo
 // next/prev ids of every node from ranks (see file comment).
 __global__ void link_kernel(const uint8_t *mi, int T, int L, long long M, Binom binom,
                             const long long *tier_first, const int32_t *rank_to_id,
-                            int32_t *next, int32_t *prev) {
+                            int32_t *next, int32_t *prev, int *bad) {
   long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   for (; i < M; i += (long long)gridDim.x * blockDim.x) {
     const uint8_t *v = mi + i * T;
@@ -195,13 +200,21 @@ __global__ void link_kernel(const uint8_t *mi, int T, int L, long long M, Binom 
     unsigned long long pre = 0;
     for (int t = 0; t < T; ++t) {
       int32_t nx = -1, pv = -1;
+      if (tier > L) {
+        atomicExch(bad, 1);
+        break;
+      }
       if (tier < L) {
         const unsigned long long r = pre + suf_up[t];
-        nx = rank_to_id[tier_first[tier + 1] + r];
+        const long long cnt = tier_first[tier + 2] - tier_first[tier + 1];
+        if (r < (unsigned long long)cnt) nx = rank_to_id[tier_first[tier + 1] + r];
+        else atomicExch(bad, 1);
       }
-      if (v[t] > 0) {
+      if (v[t] > 0 && tier > 0) {
         const unsigned long long r = pre + suf_dn[t];
-        pv = rank_to_id[tier_first[tier - 1] + r];
+        const long long cnt = tier_first[tier] - tier_first[tier - 1];
+        if (r < (unsigned long long)cnt) pv = rank_to_id[tier_first[tier - 1] + r];
+        else atomicExch(bad, 1);
       }
       next[i * T + t] = nx;
       prev[i * T + t] = pv;
@@ -266,7 +279,7 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
     return 3;
   }
 
-  DeviceBuffer d_tab, d_first_q, d_keep, d_bsum, d_total, d_tfirst;
+  DeviceBuffer d_tab, d_first_q, d_keep, d_bsum, d_total, d_tfirst, d_bad;
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
   chk(out->mi.alloc((size_t)M * T));
@@ -283,6 +296,7 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
   chk(d_keep.alloc((size_t)max_cand));
   chk(d_bsum.alloc((size_t)((max_cand + kScanBlock - 1) / kScanBlock + 1) * sizeof(long long)));
   chk(d_total.alloc(sizeof(long long)));
+  chk(d_bad.alloc(sizeof(int)));
   if (e != cudaSuccess) {
     *err = std::string("hierarchy: device allocation failed: ") + cudaGetErrorString(e);
     return 2;
@@ -294,6 +308,7 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
   uint8_t *mi = (uint8_t *)out->mi.ptr;
   int32_t *r2i = (int32_t *)out->rank_to_id.ptr;
   chk(cudaMemsetAsync(mi, 0, (size_t)T, stream));  // tier 0: the zero index
+  chk(cudaMemsetAsync(d_bad.ptr, 0, sizeof(int), stream));
   const int32_t zero = 0;
   chk(cudaMemcpyAsync(r2i, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, stream));
   chk(cudaStreamSynchronize(stream));
@@ -313,8 +328,8 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
     scan_block_sums_kernel<<<1, 1024, 0, stream>>>((long long *)d_bsum.ptr, nblk,
                                                    (long long *)d_total.ptr);
     scatter_tier_kernel<<<(unsigned)nblk, kScanBlock, 0, stream>>>(
-        mi, T, first[l - 1], C, ncand, first[l], binom, (const uint8_t *)d_keep.ptr,
-        (const long long *)d_bsum.ptr, r2i + first[l]);
+        mi, T, first[l - 1], C, ncand, first[l], count[l], binom, (const uint8_t *)d_keep.ptr,
+        (const long long *)d_bsum.ptr, r2i + first[l], d_bad.as<int>());
     long long got = 0;
     chk(cudaMemcpyAsync(&got, d_total.ptr, sizeof(long long), cudaMemcpyDeviceToHost, stream));
     chk(cudaStreamSynchronize(stream));
@@ -331,11 +346,17 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
   }
   link_kernel<<<blocks_for(M, 128), 128, 0, stream>>>(
       mi, T, L, M, binom, (const long long *)d_tfirst.ptr, r2i, (int32_t *)out->next.ptr,
-      (int32_t *)out->prev.ptr);
+      (int32_t *)out->prev.ptr, d_bad.as<int>());
   chk(cudaGetLastError());
+  int bad = 0;
+  chk(cudaMemcpyAsync(&bad, d_bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream));
   chk(cudaStreamSynchronize(stream));
   if (e != cudaSuccess) {
     *err = std::string("hierarchy: CUDA error: ") + cudaGetErrorString(e);
+    return 7;
+  }
+  if (bad) {
+    *err = "hierarchy: construction produced an index outside its tier";
     return 7;
   }
   return 0;

@@ -238,8 +238,8 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (d.truncation_level - 1 > phi::kMaxTier) return fail(nullptr, PHI_E_INVALID, "truncation_level must be <= 251");
   if (d.bath_kind < PHI_BATH_INDEPENDENT || d.bath_kind > PHI_BATH_FULL)
     return fail(nullptr, PHI_E_INVALID, "unknown bath_kind");
-  if (d.precision != PHI_PREC_FP64 && d.precision != PHI_PREC_MIXED)
-    return fail(nullptr, PHI_E_INVALID, "unknown precision");
+  if (d.precision != PHI_PREC_FP64)
+    return fail(nullptr, PHI_E_INVALID, "only PHI_PREC_FP64 is available in this build");
   if (!d.hamiltonian || !d.initial_density_matrix || !d.gamma || !d.lambda)
     return fail(nullptr, PHI_E_INVALID, "hamiltonian, initial_density_matrix, gamma and lambda are required");
   if (!(d.hbar > 0) || !(d.boltzmann_constant > 0) || !(d.temperature > 0))

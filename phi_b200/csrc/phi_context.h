@@ -52,8 +52,17 @@ struct phi_ctx {
   cudaGraphExec_t rkf45_graph = nullptr;
   int rkf45_graph_steps = 0;
 
+  // RKF45 state kept between calls (phi_gpu_rkf45_advance with dt0 <= 0).
+  phi::Rkf45Ctl rkf45_last{};
+  bool rkf45_started = false;
+  void *host_ctl = nullptr;        // pinned copy of the control block
+  long long graph_launches = 0;    // step graphs launched so far
+
   double time = 0.0;
   std::string error;
+  ~phi_ctx() {
+    if (host_ctl) cudaFreeHost(host_ctl);
+  }
 
   size_t state_bytes() const {
     return (size_t)hier.M * desc.num_states * desc.num_states * sizeof(double2);

@@ -214,29 +214,40 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
   return PHI_OK;
 }
 
-extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
-                             int64_t max_steps, phi_rkf45_stats *stats) {
-  if (!ctx) return PHI_E_INVALID;
-  if (!(dt0 > 0) || !(tol > 0) || !(min_dt > 0) || !std::isfinite(t_end)) {
+namespace {
+
+// Shared driver of phi_gpu_rkf45 / phi_gpu_rkf45_advance.
+int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
+              int64_t max_steps, bool limit_is_error, phi_rkf45_stats *stats) {
+  if (!(tol > 0) || !(min_dt > 0) || !std::isfinite(t_end) || (limit_is_error && !(dt0 > 0))) {
     ctx->error = "rkf45: dt0, tol and min_dt must be positive and t_end finite";
     return PHI_E_INVALID;
+  }
+  const bool resume = !(dt0 > 0);
+  if (resume && !ctx->rkf45_started) {
+    ctx->error = "rkf45: dt0 <= 0 continues a previous run, but there is none";
+    return PHI_E_STATE;
   }
   int rc = ctx->ensure_work(3);
   if (rc != PHI_OK) return rc;
   phi::Rkf45Ctl hc{};
+  if (resume) {
+    hc = ctx->rkf45_last;
+  } else {
+    hc.dt = dt0;
+    hc.dtup = 1.1;
+    hc.dtdn = 0.5;
+    // Butcher tableau of Rkf45Integrate (:1937-1975), each entry scaled by dt0.
+    const double tab[24] = {2. / 9.,   1. / 12.,  1. / 4.,   69. / 128., -243. / 128., 135. / 64.,
+                            -17. / 12., 27. / 4.,  -27. / 5,  16. / 15,   65. / 432.,   -5. / 16,
+                            13. / 16.,  4. / 27.,  5. / 144., 1. / 9,     9. / 20,      16. / 45,
+                            1. / 12,    47. / 450, 12. / 25,  32. / 225,  1. / 30,      6. / 25};
+    for (int q = 0; q < 24; ++q) hc.coef[q] = tab[q] * dt0;
+  }
   hc.time = ctx->time;
   hc.end_time = t_end;
-  hc.dt = dt0;
   hc.tol = tol;
   hc.min_dt = min_dt;
-  hc.dtup = 1.1;
-  hc.dtdn = 0.5;
-  // Butcher tableau of Rkf45Integrate (:1937-1975), each entry scaled by dt0.
-  const double tab[24] = {2. / 9.,   1. / 12.,  1. / 4.,   69. / 128., -243. / 128., 135. / 64.,
-                          -17. / 12., 27. / 4.,  -27. / 5,  16. / 15,   65. / 432.,   -5. / 16,
-                          13. / 16.,  4. / 27.,  5. / 144., 1. / 9,     9. / 20,      16. / 45,
-                          1. / 12,    47. / 450, 12. / 25,  32. / 225,  1. / 30,      6. / 25};
-  for (int q = 0; q < 24; ++q) hc.coef[q] = tab[q] * dt0;
   hc.max_error = 0.0;
   hc.err_bits = 0ull;
   hc.steps = 0;
@@ -256,14 +267,20 @@ extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol,
       return cudaSuccess;
     }, &ctx->rkf45_graph));
   }
-  phi::Rkf45Ctl *hpin = nullptr;
-  PHI_CK(cudaMallocHost(&hpin, sizeof(phi::Rkf45Ctl)));
+  if (!ctx->host_ctl) PHI_CK(cudaMallocHost(&ctx->host_ctl, sizeof(phi::Rkf45Ctl)));
+  phi::Rkf45Ctl *hpin = static_cast<phi::Rkf45Ctl *>(ctx->host_ctl);
   int result = PHI_OK;
   // Two graphs in flight: the done flag of launch j is read while launch j+1
   // runs; steps after completion are no-ops on the device.
+  long long launched = 0;
   PHI_CK(cudaGraphLaunch(ctx->rkf45_graph, ctx->stream));
+  launched += kGraphSteps;
   for (;;) {
-    cudaError_t e = cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
+    cudaError_t e = cudaSuccess;
+    if (launched < hc.max_steps) {
+      e = cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
+      launched += kGraphSteps;
+    }
     if (e == cudaSuccess) e = cudaMemcpyAsync(hpin, ctx->ctl.ptr, sizeof(phi::Rkf45Ctl), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
@@ -272,10 +289,16 @@ extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol,
     }
     if (hpin->done) break;
   }
+  ctx->graph_launches += launched / kGraphSteps;
   if (result == PHI_OK) {
     hc = *hpin;
-    if (hc.ycur == 1) std::swap(ctx->y, ctx->y_alt);
+    if (hc.ycur == 1) {
+      std::swap(ctx->y, ctx->y_alt);
+      ctx->release_graphs();  // captured graphs bake in the y / y_alt pointers
+    }
     ctx->time = hc.time;
+    ctx->rkf45_last = hc;
+    ctx->rkf45_started = true;
     if (stats) {
       stats->steps = hc.steps;
       stats->accepted = hc.accepted;
@@ -283,7 +306,7 @@ extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol,
       stats->final_dt = hc.dt;
       stats->max_error = hc.max_error;
     }
-    if (hc.status == 1) {
+    if (hc.status == 1 && limit_is_error) {
       ctx->error = "rkf45: step limit reached before t_end";
       result = PHI_E_STEP_COLLAPSE;
     } else if (hc.status == 2) {
@@ -291,8 +314,29 @@ extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol,
       result = PHI_E_NUMERIC;
     }
   }
-  cudaFreeHost(hpin);
-  // Captured graphs bake in the y / y_alt pointers; a swap invalidates them.
-  if (hc.ycur == 1) ctx->release_graphs();
   return result;
+}
+
+}  // namespace
+
+extern "C" int phi_gpu_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
+                             int64_t max_steps, phi_rkf45_stats *stats) {
+  if (!ctx) return PHI_E_INVALID;
+  return run_rkf45(ctx, dt0, t_end, tol, min_dt, max_steps, true, stats);
+}
+
+extern "C" int phi_gpu_rkf45_advance(phi_ctx *ctx, double dt0, double t_end, double tol,
+                                     double min_dt, int64_t steps, phi_rkf45_stats *stats) {
+  if (!ctx) return PHI_E_INVALID;
+  if (steps <= 0) {
+    ctx->error = "rkf45_advance: steps must be positive";
+    return PHI_E_INVALID;
+  }
+  return run_rkf45(ctx, dt0, t_end, tol, min_dt, steps, false, stats);
+}
+
+extern "C" int phi_gpu_stream(const phi_ctx *ctx, void **stream) {
+  if (!ctx || !stream) return PHI_E_INVALID;
+  *stream = (void *)ctx->stream;
+  return PHI_OK;
 }

@@ -234,3 +234,16 @@ class Hierarchy:
                                            float(min_dt), int(max_steps), ctypes.byref(st)))
         return {"steps": st.steps, "accepted": st.accepted, "final_time": st.final_time,
                 "final_dt": st.final_dt, "max_error": st.max_error}
+
+    def rkf45_advance(self, dt0: float, t_end: float, tol: float, min_dt: float, steps: int):
+        """Exactly `steps` attempted steps (fewer at t_end); dt0 <= 0 continues."""
+        st = capi.PhiRkf45Stats()
+        self._check(self.lib.phi_gpu_rkf45_advance(self.ctx, float(dt0), float(t_end), float(tol),
+                                                   float(min_dt), int(steps), ctypes.byref(st)))
+        return {"steps": st.steps, "accepted": st.accepted, "final_time": st.final_time,
+                "final_dt": st.final_dt, "max_error": st.max_error}
+
+    def stream_handle(self) -> int:
+        s = ctypes.c_void_p()
+        self._check(self.lib.phi_gpu_stream(self.ctx, ctypes.byref(s)))
+        return s.value or 0
