@@ -185,6 +185,20 @@ PHI_API int phi_gpu_stream(const phi_ctx *ctx, void **stream);
 PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);
 PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);
 
+/* One RK4 step that allocates no memory, for callers that cannot call
+ * cudaMalloc when they step (code under stream capture, hosts that own all
+ * device memory through their own allocator, latency-bound loops).  No
+ * counterpart in the reference.  d_in and d_out are distinct caller-owned
+ * device buffers of M*N*N complex128 (node-major); d_out receives the state
+ * one step of size dt after d_in, d_in is not modified; the work runs on
+ * `stream` (a cudaStream_t) and the call returns without synchronising.  The
+ * two stage-input buffers live in a built-in 16 MiB device array, so the
+ * state may be at most 8 MiB (PHI_E_INVALID above that); all calls share
+ * that array, so calls that overlap on the GPU race.  The first call on a
+ * device looks up the array's address; make it before any stream capture. */
+PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out, double dt,
+                                     void *stream);
+
 /* Copies the text of the last error on this context (or of the last failed
  * create when ctx is NULL) into buf. */
 PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
