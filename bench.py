@@ -6,6 +6,11 @@ One bench "step" is one attempted RKF45 step over the whole hierarchy: six
 fused Liouvillian-apply + stage-combine kernels over all 38,760 nodes, the
 error max-reduction and the device-side accept/step-size control.
 
+The headline arithmetic is the mixed mode (complex64 stage inputs and
+derivatives, FP32 Liouvillian, FP64 state / combines / error norm / step
+control); the same run times the FP64 path and integrates the full 1 ps in
+both to report the max-abs rho_0 error of the mixed mode against FP64.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl phi_b200|reference]
                     [--precision fp64|mixed]
 
@@ -43,7 +48,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=16)
     ap.add_argument("--impl", default="phi_b200", choices=["phi_b200", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -261,7 +266,11 @@ def main():
 
     # ---- dominant kernel in isolation: one apply launch over all nodes ----
     E = N * N
-    x = torch.randn(M * E * 2, dtype=torch.float64, device="cuda")
+    EPX = (E + (E & 1)) if prec == capi.PHI_PREC_MIXED else E
+    if prec == capi.PHI_PREC_MIXED:
+        x = torch.randn(M * EPX * 2, dtype=torch.float32, device="cuda")
+    else:
+        x = torch.randn(M * E * 2, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
     reps = 20
     with torch.cuda.stream(stream):
@@ -295,12 +304,37 @@ def main():
     h2d = (2 * E + 2 * E + 2 * 7) * 8  # H, rho(0), gamma, lambda
     d2h = 2 * E * 8 + ((e2e_steps + 15) // 16 + 1) * 320  # rho_0 + control-block polls
 
+    # ---- the other arithmetic, and the full 1 ps rho_0 error of mixed vs FP64 ----
+    other = capi.PHI_PREC_FP64 if prec == capi.PHI_PREC_MIXED else capi.PHI_PREC_MIXED
+    ho = Hierarchy(p, precision=other, device=local_rank)
+    so = torch.cuda.ExternalStream(ho.stream_handle(), device=local_rank)
+    ho.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup)
+    torch.cuda.synchronize()
+    e0o, e1o = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0o.record(so)
+    sto = ho.rkf45_advance(-1.0, T_END, TOL, MIN_DT, args.steps)
+    e1o.record(so)
+    e1o.synchronize()
+    other_ms_per_step = e0o.elapsed_time(e1o) / max(int(sto["steps"]), 1)
+    ho.close()
+    rho_full = {}
+    for pr in (capi.PHI_PREC_FP64, capi.PHI_PREC_MIXED):
+        hf = Hierarchy(p, precision=pr, device=local_rank)
+        stf = hf.rkf45(DT0, T_END, TOL, MIN_DT)
+        rho_full[pr] = (hf.rho0(), stf)
+        hf.close()
+    rho_err = float(np.abs(rho_full[capi.PHI_PREC_MIXED][0] - rho_full[capi.PHI_PREC_FP64][0]).max())
+
     if rank == 0:
         peak, peak_kind = peaks()
         S = M * E * 16
-        step_bytes = 36 * S           # fused RKF45 step
+        EP = E + (E & 1)
+        # Algorithmic bytes of one fused RKF45 step: FP64 touches
+        # 36 complex128 state-size arrays; mixed touches 7 complex128 (y reads,
+        # y5 write) and 31 complex64 ones (stage inputs, k, y32).
+        step_bytes = 36 * S if prec == capi.PHI_PREC_FP64 else M * (7 * E * 16 + 31 * EP * 8)
         achieved = step_bytes / (ms_per_step / 1e3) / 1e9
-        apply_bytes = 2 * S
+        apply_bytes = 2 * S if prec == capi.PHI_PREC_FP64 else 2 * M * EPX * 8
         apply_gbs = apply_bytes / (apply_ms / 1e3) / 1e9
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
@@ -313,7 +347,7 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "c128" if prec == capi.PHI_PREC_FP64 else "c64+c128",
+            "dtype": "c128" if prec == capi.PHI_PREC_FP64 else "c64 stages (fp32 Liouvillian) + c128 state/norms",
             "data": "synthetic (seeded frenkel7, numpy default_rng seed 7)",
             "config": {"workload": "frenkel7_K1_L6: 7-site Frenkel exciton, 7 Drude baths, K=1, L=6, "
                                    "38760 nodes of 7x7, RKF45 tol 1e-6 to 1 ps",
@@ -321,10 +355,20 @@ def main():
                        "precision": args.precision, "parallelism": f"replicas x{world}",
                        "l2": "working set 9 x 30.4 MB state buffers = 274 MB > 126 MB L2"},
             "rkf45_steps_per_s": total_steps / (t_max / 1e3),
+            "rho0_err_vs_fp64": rho_err,
+            "meets_1e-6": rho_err <= 1e-6,
+            "full_run": {"t_end_ps": T_END,
+                         "fp64_steps": int(rho_full[capi.PHI_PREC_FP64][1]["steps"]),
+                         "mixed_steps": int(rho_full[capi.PHI_PREC_MIXED][1]["steps"])},
+            "other_precision": {"precision": "fp64" if other == capi.PHI_PREC_FP64 else "mixed",
+                                "ms_per_step": other_ms_per_step,
+                                "value": 6 * M / (other_ms_per_step / 1e3)},
+            "speedup_vs_fp64": (other_ms_per_step / ms_per_step) if other == capi.PHI_PREC_FP64 else
+                               (ms_per_step / other_ms_per_step),
             "steps_timed": steps_done,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "kernel": "heom_stage_kernel x6 + rkf45_control (one RKF45 step)",
+                         "kernel": "heom_tile_kernel x6 + rkf45_control_kernel (one RKF45 step)",
                          "algorithmic_bytes_per_step": step_bytes, "peak_kind": peak_kind},
             "apply_kernel": {"ms": apply_ms, "algorithmic_bytes": apply_bytes, "achieved_gbs": apply_gbs,
                              "frac": apply_gbs / peak, "node_applies_per_s": M / (apply_ms / 1e3)},

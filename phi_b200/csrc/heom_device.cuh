@@ -31,6 +31,7 @@ struct HeomConsts {
   int L;            // deepest tier (truncation_level - 1)
   int kind;         // BathKind
   int vacuum;       // truncation_level == 1: unitary part only
+  int identity_sites;  // independent baths: bath m couples to |m><m|
   int64_t M;        // nodes
   double inv_hbar;  // 1 / hbar
   const uint8_t *mi;     // M*T
@@ -49,6 +50,7 @@ struct HeomConsts {
   const double *mats_bath;   // nb: Delta_b
   const uint8_t *pair_i;     // N(N+1)/2 upper-triangle pairs (i <= j)
   const uint8_t *pair_j;
+  int *err_flag;             // set by a kernel whose bounded wait gave up
 };
 
 // Device control block of the adaptive integrator; lives in device memory and

@@ -28,6 +28,7 @@
 
 #include "heom_device.cuh"
 #include "heom_kernels.h"
+#include "heom_tile.h"
 
 namespace phi {
 namespace {
@@ -493,6 +494,15 @@ int stage_grid(const HeomConsts &c, int num_sms) {
 }
 
 cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream) {
+  if (tile_kernel_available(L.c)) {
+    if (L.xv || L.outv || L.mixed) return launch_tile_stage(L, stream);
+    StageLaunch T = L;  // complex128 caller: the typed pointers are the storage
+    T.xv = L.x;
+    T.outv = L.out;
+    for (int i = 0; i < 5; ++i) T.kv[i] = L.k[i];
+    return launch_tile_stage(T, stream);
+  }
+  if (L.mixed) return cudaErrorInvalidValue;  // mixed precision needs the tiled kernel
   StageParams p;
   p.c = L.c;
   p.mode = L.mode;
@@ -526,6 +536,43 @@ cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream) {
     PHI_DISPATCH(256)
   }
 #undef PHI_DISPATCH
+}
+
+namespace {
+__global__ void to_c64_kernel(const double2 *in, float2 *out, long long M, int E, int EP) {
+  const long long total = M * EP;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long n = i / EP;
+    const int w = (int)(i - n * EP);
+    const double2 v = w < E ? in[n * E + w] : make_double2(0.0, 0.0);
+    out[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+__global__ void to_c128_kernel(const float2 *in, double2 *out, long long M, int E, int EP) {
+  const long long total = M * E;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long n = i / E;
+    const int w = (int)(i - n * E);
+    const float2 v = in[n * EP + w];
+    out[i] = make_double2(v.x, v.y);
+  }
+}
+int conv_blocks(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b < 1 ? 1 : (b > 148 * 16 ? 148 * 16 : b));
+}
+}  // namespace
+
+cudaError_t launch_to_c64(const double2 *in, float2 *out, long long M, int E, int padded, cudaStream_t s) {
+  to_c64_kernel<<<conv_blocks(M * padded), 256, 0, s>>>(in, out, M, E, padded);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_to_c128(const float2 *in, double2 *out, long long M, int E, int padded, cudaStream_t s) {
+  to_c128_kernel<<<conv_blocks(M * E), 256, 0, s>>>(in, out, M, E, padded);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_rkf45_control(Rkf45Ctl *ctl, cudaStream_t stream) {

@@ -26,6 +26,15 @@ struct StageLaunch {
   double2 *k[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RKF45 k0..k4
   double2 *ybuf[2] = {nullptr, nullptr};                          // RKF45 state ping-pong
   Rkf45Ctl *ctl = nullptr;
+  // Tiled kernel: stage input / output and k buffers in the context's
+  // storage type (complex128, or complex64 in mixed precision), the
+  // complex64 copies of the state, and the arithmetic.
+  bool mixed = false;
+  const void *xv = nullptr;
+  void *outv = nullptr;
+  void *kv[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  void *y32 = nullptr;
+  void *y32buf[2] = {nullptr, nullptr};
 };
 
 int choose_group(int N);
@@ -33,5 +42,8 @@ size_t stage_smem_bytes(int N, int T, int kind);
 int stage_grid(const HeomConsts &c, int num_sms);
 cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream);
 cudaError_t launch_rkf45_control(Rkf45Ctl *ctl, cudaStream_t stream);
+// complex128 (node stride N*N) <-> complex64 (node stride `padded`).
+cudaError_t launch_to_c64(const double2 *in, float2 *out, long long M, int E, int padded, cudaStream_t s);
+cudaError_t launch_to_c128(const float2 *in, double2 *out, long long M, int E, int padded, cudaStream_t s);
 
 }  // namespace phi

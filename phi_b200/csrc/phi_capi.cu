@@ -18,6 +18,7 @@
 #include "heom_device.cuh"
 #include "heom_internal.h"
 #include "heom_kernels.h"
+#include "heom_tile.h"
 #include "phi_context.h"
 
 using phi::DeviceBuffer;
@@ -185,6 +186,8 @@ int setup_constants(phi_ctx *ctx) {
   chk(upload(cb.mats_bath, delta, s));
   chk(upload(cb.pair_i, pi, s));
   chk(upload(cb.pair_j, pj, s));
+  chk(cb.err_flag.alloc(sizeof(int)));
+  chk(cudaMemsetAsync(cb.err_flag.ptr, 0, sizeof(int), s));
   chk(cudaStreamSynchronize(s));
   if (e != cudaSuccess) return cuda_fail(ctx, e, "constant upload");
 
@@ -196,6 +199,12 @@ int setup_constants(phi_ctx *ctx) {
   c.L = L;
   c.kind = d.bath_kind;
   c.vacuum = vacuum ? 1 : 0;
+  c.identity_sites = 0;
+  if (d.bath_kind == PHI_BATH_INDEPENDENT && nb == N) {
+    c.identity_sites = 1;
+    for (int b = 0; b < nb; ++b)
+      if (ctx->bath_sites[b] != b) c.identity_sites = 0;
+  }
   c.M = ctx->hier.M;
   c.inv_hbar = 1.0 / hbar;
   c.mi = ctx->hier.mi.as<uint8_t>();
@@ -214,6 +223,7 @@ int setup_constants(phi_ctx *ctx) {
   c.mats_bath = cb.mats_bath.as<double>();
   c.pair_i = cb.pair_i.as<uint8_t>();
   c.pair_j = cb.pair_j.as<uint8_t>();
+  c.err_flag = cb.err_flag.as<int>();
   return PHI_OK;
 }
 
@@ -238,8 +248,8 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (d.truncation_level - 1 > phi::kMaxTier) return fail(nullptr, PHI_E_INVALID, "truncation_level must be <= 251");
   if (d.bath_kind < PHI_BATH_INDEPENDENT || d.bath_kind > PHI_BATH_FULL)
     return fail(nullptr, PHI_E_INVALID, "unknown bath_kind");
-  if (d.precision != PHI_PREC_FP64)
-    return fail(nullptr, PHI_E_INVALID, "only PHI_PREC_FP64 is available in this build");
+  if (d.precision != PHI_PREC_FP64 && d.precision != PHI_PREC_MIXED)
+    return fail(nullptr, PHI_E_INVALID, "unknown precision");
   if (!d.hamiltonian || !d.initial_density_matrix || !d.gamma || !d.lambda)
     return fail(nullptr, PHI_E_INVALID, "hamiltonian, initial_density_matrix, gamma and lambda are required");
   if (!(d.hbar > 0) || !(d.boltzmann_constant > 0) || !(d.temperature > 0))
@@ -317,6 +327,10 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
     g_create_error = ctx->error;
     return rc;
   }
+  if (d.precision == PHI_PREC_MIXED && !phi::tile_kernel_available(ctx->c))
+    return fail(nullptr, PHI_E_INVALID,
+                "mixed precision is built for independent baths on PHI's identity site map, K+1 <= 3 and "
+                "N in {2..8, 10, 12, 16, 24}");
   ctx->grid = phi::stage_grid(ctx->c, ctx->num_sms);
   const size_t state_bytes = (size_t)ctx->hier.M * N * N * sizeof(double2);
   e = ctx->y.alloc(state_bytes);
@@ -394,29 +408,62 @@ extern "C" int phi_gpu_get_rho0(const phi_ctx *cctx, double *rho0) {
   return PHI_OK;
 }
 
+int phi_ctx::check_device_flag() {
+  int flag = 0;
+  cudaError_t e = cudaMemcpyAsync(&flag, cbuf.err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  if (e != cudaSuccess) return cuda_fail(this, e, "device flag read");
+  if (flag) {
+    cudaMemsetAsync(cbuf.err_flag.ptr, 0, sizeof(int), stream);
+    error = "a device wait on a bulk copy gave up (bounded mbarrier wait)";
+    return PHI_E_TIMEOUT;
+  }
+  return PHI_OK;
+}
+
 extern "C" int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream) {
   if (!ctx || !d_in || !d_out) return PHI_E_INVALID;
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15u) {
+    ctx->error = "apply_device: device buffers must be 16-byte aligned";
+    return PHI_E_INVALID;
+  }
   phi::StageLaunch L;
   L.c = ctx->c;
   L.mode = phi::kModeApply;
   L.grid = ctx->grid;
   L.x = static_cast<const double2 *>(d_in);
   L.out = static_cast<double2 *>(d_out);
+  L.xv = d_in;
+  L.outv = d_out;
+  L.mixed = ctx->mixed();
   PHI_CUDA(ctx, phi::launch_stage(L, static_cast<cudaStream_t>(stream)));
   return PHI_OK;
 }
 
 extern "C" int phi_gpu_apply(phi_ctx *ctx, const double *in, double *out) {
   if (!ctx || !in || !out) return PHI_E_INVALID;
-  int rc = ctx->ensure_work(1);
+  int rc = ctx->ensure_work(ctx->mixed() ? 2 : 1);
   if (rc != PHI_OK) return rc;
   const size_t b = ctx->state_bytes();
-  PHI_CUDA(ctx, cudaMemcpyAsync(ctx->xa.ptr, in, b, cudaMemcpyHostToDevice, ctx->stream));
+  const int E = ctx->desc.num_states * ctx->desc.num_states;
+  if (ctx->mixed()) {  // complex128 host data through the complex64 stage buffers
+    PHI_CUDA(ctx, cudaMemcpyAsync(ctx->acc.ptr, in, b, cudaMemcpyHostToDevice, ctx->stream));
+    PHI_CUDA(ctx, phi::launch_to_c64(ctx->acc.as<double2>(), ctx->xa.as<float2>(), ctx->hier.M, E,
+                                     ctx->work_stride(), ctx->stream));
+  } else {
+    PHI_CUDA(ctx, cudaMemcpyAsync(ctx->xa.ptr, in, b, cudaMemcpyHostToDevice, ctx->stream));
+  }
   rc = phi_gpu_apply_device(ctx, ctx->xa.ptr, ctx->xb.ptr, ctx->stream);
   if (rc != PHI_OK) return rc;
-  PHI_CUDA(ctx, cudaMemcpyAsync(out, ctx->xb.ptr, b, cudaMemcpyDeviceToHost, ctx->stream));
+  if (ctx->mixed()) {
+    PHI_CUDA(ctx, phi::launch_to_c128(ctx->xb.as<float2>(), ctx->acc.as<double2>(), ctx->hier.M, E,
+                                      ctx->work_stride(), ctx->stream));
+    PHI_CUDA(ctx, cudaMemcpyAsync(out, ctx->acc.ptr, b, cudaMemcpyDeviceToHost, ctx->stream));
+  } else {
+    PHI_CUDA(ctx, cudaMemcpyAsync(out, ctx->xb.ptr, b, cudaMemcpyDeviceToHost, ctx->stream));
+  }
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  return PHI_OK;
+  return ctx->check_device_flag();
 }
 
 extern "C" int phi_gpu_get_time(const phi_ctx *ctx, double *time) {

@@ -14,7 +14,7 @@
 // Device copies of the per-term / per-element constants (HeomConsts points here).
 struct PhiConstBuffers {
   phi::DeviceBuffer H, corr, nu, sq_next, sq_prev, term_site, site_ptr, site_terms,
-      mats_elem, bath_V, mats_bath, pair_i, pair_j;
+      mats_elem, bath_V, mats_bath, pair_i, pair_j, err_flag;
 };
 
 struct phi_ctx {
@@ -34,9 +34,13 @@ struct phi_ctx {
   PhiConstBuffers cbuf;
   phi::HeomConsts c{};
 
-  // State and integrator work space (node-major, complex128).
+  // State and integrator work space (node-major).  y, y_alt and acc are
+  // complex128; the stage inputs and k buffers are complex128, or complex64
+  // with the node stride padded to even in mixed precision, where y32 /
+  // y32_alt hold complex64 copies of y / y_alt.
   phi::DeviceBuffer y;         // current state
   phi::DeviceBuffer y_alt;     // RKF45 candidate state
+  phi::DeviceBuffer y32, y32_alt;
   phi::DeviceBuffer xa, xb;    // stage inputs (ping-pong)
   phi::DeviceBuffer acc;       // RK4 accumulator
   phi::DeviceBuffer kbuf[5];   // RKF45 k0..k4
@@ -67,8 +71,14 @@ struct phi_ctx {
   size_t state_bytes() const {
     return (size_t)hier.M * desc.num_states * desc.num_states * sizeof(double2);
   }
+  bool mixed() const { return desc.precision == PHI_PREC_MIXED; }
+  // Node stride (elements) and bytes of the stage / k buffers.
+  int work_stride() const;
+  size_t work_bytes() const;
   int ensure_work(int level);
   void release_graphs();
+  // PHI_E_TIMEOUT if a kernel's bounded wait gave up since the last check.
+  int check_device_flag();
 };
 
 namespace phi {

@@ -20,6 +20,7 @@
 
 #include "../../include/phi_b200.h"
 #include "heom_kernels.h"
+#include "heom_tile.h"
 #include "phi_context.h"
 
 namespace {
@@ -39,18 +40,29 @@ constexpr int kGraphSteps = 16;
 
 }  // namespace
 
+int phi_ctx::work_stride() const {
+  const int N = desc.num_states;
+  return mixed() ? phi::mixed_node_stride(N) : N * N;
+}
+
+size_t phi_ctx::work_bytes() const {
+  return (size_t)hier.M * work_stride() * (mixed() ? sizeof(float2) : sizeof(double2));
+}
+
 int phi_ctx::ensure_work(int level) {
-  const size_t b = state_bytes();
-  auto alloc = [&](phi::DeviceBuffer &buf) -> bool {
+  const size_t b = state_bytes(), wb = work_bytes();
+  auto alloc = [&](phi::DeviceBuffer &buf, size_t bytes) -> bool {
     if (buf.ptr) return true;
-    return buf.alloc(b) == cudaSuccess;
+    return buf.alloc(bytes) == cudaSuccess;
   };
   bool ok = true;
-  if (level >= 1) ok = ok && alloc(xa) && alloc(xb);
-  if (level >= 2) ok = ok && alloc(acc);
+  if (level >= 1) ok = ok && alloc(xa, wb) && alloc(xb, wb);
+  if (level >= 2) ok = ok && alloc(acc, b);
+  if (level >= 2 && mixed()) ok = ok && alloc(y32, wb);
   if (level >= 3) {
-    ok = ok && alloc(y_alt);
-    for (auto &k : kbuf) ok = ok && alloc(k);
+    ok = ok && alloc(y_alt, b);
+    if (mixed()) ok = ok && alloc(y32_alt, wb);
+    for (auto &k : kbuf) ok = ok && alloc(k, wb);
   }
   if (ok && !ctl.ptr) ok = ctl.alloc(std::max(sizeof(phi::Rkf45Ctl), sizeof(phi::Rk4Ctl))) == cudaSuccess;
   if (!ok) {
@@ -80,15 +92,21 @@ cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, cudaStream_
   L.acc = ctx->acc.as<double2>();
   L.rk4 = ctx->ctl.as<phi::Rk4Ctl>();
   L.traj = traj;
+  L.mixed = ctx->mixed();
+  L.y32 = ctx->y32.ptr;
   double2 *xa = ctx->xa.as<double2>(), *xb = ctx->xb.as<double2>();
   const double a[4] = {dt / 2, dt / 2, dt, 0.0};
   const double w[4] = {dt / 6, dt / 3, dt / 3, dt / 6};
   const double2 *in[4] = {L.y, xa, xb, xa};
   double2 *outb[4] = {xa, xb, xa, nullptr};
+  const void *inv[4] = {L.mixed ? ctx->y32.ptr : (const void *)L.y, ctx->xa.ptr, ctx->xb.ptr, ctx->xa.ptr};
+  void *outv[4] = {ctx->xa.ptr, ctx->xb.ptr, ctx->xa.ptr, nullptr};
   for (int st = 0; st < 4; ++st) {
     L.stage = st;
     L.x = in[st];
     L.out = outb[st];
+    L.xv = inv[st];
+    L.outv = outv[st];
     L.a_next = a[st];
     L.w_acc = w[st];
     cudaError_t e = phi::launch_stage(L, s);
@@ -105,7 +123,13 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
   L.ctl = ctx->ctl.as<phi::Rkf45Ctl>();
   L.ybuf[0] = ctx->y.as<double2>();
   L.ybuf[1] = ctx->y_alt.as<double2>();
-  for (int i = 0; i < 5; ++i) L.k[i] = ctx->kbuf[i].as<double2>();
+  L.mixed = ctx->mixed();
+  L.y32buf[0] = ctx->y32.ptr;
+  L.y32buf[1] = ctx->y32_alt.ptr;
+  for (int i = 0; i < 5; ++i) {
+    L.k[i] = ctx->kbuf[i].as<double2>();
+    L.kv[i] = ctx->kbuf[i].ptr;
+  }
   double2 *xa = ctx->xa.as<double2>(), *xb = ctx->xb.as<double2>();
   const double2 *in[6] = {nullptr, xa, xb, xa, xb, xa};
   double2 *outb[6] = {xa, xb, xa, xb, xa, nullptr};
@@ -113,6 +137,8 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
     L.stage = st;
     L.x = in[st];
     L.out = outb[st];
+    L.xv = in[st];
+    L.outv = outb[st];
     cudaError_t e = phi::launch_stage(L, s);
     if (e != cudaSuccess) return e;
   }
@@ -173,6 +199,9 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
     }
     dtraj = ctx->traj.as<double2>();
   }
+  if (ctx->mixed())
+    PHI_CK(phi::launch_to_c64(ctx->y.as<double2>(), ctx->y32.as<float2>(), ctx->hier.M,
+                              ctx->desc.num_states * ctx->desc.num_states, ctx->work_stride(), ctx->stream));
   phi::Rk4Ctl hc{};
   hc.step = 0;
   hc.out_factor = out_factor;
@@ -211,7 +240,7 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
   ctx->time = t;
   if (num_steps) *num_steps = steps;
   if (num_out) *num_out = (int64_t)out_times.size();
-  return PHI_OK;
+  return ctx->check_device_flag();
 }
 
 namespace {
@@ -258,6 +287,9 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
   hc.status = 0;
   hc.nonfinite = 0;
   PHI_CK(cudaMemcpyAsync(ctx->ctl.ptr, &hc, sizeof(hc), cudaMemcpyHostToDevice, ctx->stream));
+  if (ctx->mixed())  // stage-0 input of the first step: complex64 copy of y (ycur = 0)
+    PHI_CK(phi::launch_to_c64(ctx->y.as<double2>(), ctx->y32.as<float2>(), ctx->hier.M,
+                              ctx->desc.num_states * ctx->desc.num_states, ctx->work_stride(), ctx->stream));
   if (!ctx->rkf45_graph) {
     PHI_CK(capture(ctx->stream, [&]() {
       for (int i = 0; i < kGraphSteps; ++i) {
@@ -294,6 +326,7 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
     hc = *hpin;
     if (hc.ycur == 1) {
       std::swap(ctx->y, ctx->y_alt);
+      std::swap(ctx->y32, ctx->y32_alt);
       ctx->release_graphs();  // captured graphs bake in the y / y_alt pointers
     }
     ctx->time = hc.time;
@@ -314,6 +347,7 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
       result = PHI_E_NUMERIC;
     }
   }
+  if (result == PHI_OK) result = ctx->check_device_flag();
   return result;
 }
 

@@ -67,6 +67,14 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
     ctx->error = "rk4_step_noalloc: needs distinct non-NULL input and output buffers and dt > 0";
     return PHI_E_INVALID;
   }
+  if ((reinterpret_cast<uintptr_t>(d_in) | reinterpret_cast<uintptr_t>(d_out)) & 15u) {
+    ctx->error = "rk4_step_noalloc: device buffers must be 16-byte aligned";
+    return PHI_E_INVALID;
+  }
+  if (ctx->mixed()) {
+    ctx->error = "rk4_step_noalloc: complex128 (PHI_PREC_FP64) contexts only";
+    return PHI_E_INVALID;
+  }
   const size_t bytes = ctx->state_bytes();
   if (bytes > kNoAllocMaxStateBytes) {
     ctx->error = "rk4_step_noalloc: hierarchy state of " + std::to_string(bytes) +
