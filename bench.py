@@ -45,7 +45,7 @@ MIN_DT = 1e-6
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=16)
     ap.add_argument("--impl", default="phi_b200", choices=["phi_b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
@@ -92,6 +92,11 @@ class ClockSampler:
             self.thread.start()
         except Exception:
             self.proc = None
+
+    def wait_first_sample(self, timeout=5.0):
+        t0 = time.time()
+        while self.proc and not self.lines and time.time() - t0 < timeout:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:
@@ -201,6 +206,23 @@ def run_reference_arm(args):
     return res
 
 
+def run_steps(h, steps, fresh):
+    """Exactly `steps` attempted RKF45 steps of the 1 ps propagation; when a
+    propagation reaches t_end it restarts from rho(0) on the device
+    (phi_gpu_reset).  Returns (steps, propagations finished)."""
+    done = finished = 0
+    dt0 = DT0 if fresh else -1.0
+    while done < steps:
+        st = h.rkf45_advance(dt0, T_END, TOL, MIN_DT, steps - done)
+        done += int(st["steps"])
+        dt0 = -1.0
+        if st["final_time"] >= T_END:
+            h.reset(0.0)
+            finished += 1
+            dt0 = DT0
+    return done, finished
+
+
 def main():
     args = parse_args()
     if args.warmup < 3:
@@ -233,23 +255,23 @@ def main():
     h = Hierarchy(p, precision=prec, device=local_rank)
     M = h.num_nodes
     stream = torch.cuda.ExternalStream(h.stream_handle(), device=local_rank)
-    h.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup)
+    run_steps(h, args.warmup, True)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     sampler = ClockSampler(local_rank)
     sampler.start()
+    sampler.wait_first_sample()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
-    st = h.rkf45_advance(-1.0, T_END, TOL, MIN_DT, args.steps)
+    steps_done, propagations = run_steps(h, args.steps, False)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = ev0.elapsed_time(ev1)
-    steps_done = int(st["steps"])
     t_max = ms
     if dist:
         t = torch.tensor([ms], device="cuda")
@@ -289,12 +311,16 @@ def main():
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
-    h2 = Hierarchy(p, precision=prec, device=local_rank)
-    st2 = h2.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup + args.steps)
-    rho0 = h2.rho0()
-    h2.close()
-    e2e_s = time.perf_counter() - t0
+    # The user job: build the hierarchy on the device from host arrays, run the
+    # whole 1 ps RKF45 propagation, read rho_0 back, tear down.  Run twice in
+    # this warm process; the second run is reported.
+    for _ in range(2):
+        t0 = time.perf_counter()
+        h2 = Hierarchy(p, precision=prec, device=local_rank)
+        st2 = h2.rkf45(DT0, T_END, TOL, MIN_DT)
+        rho0 = h2.rho0()
+        h2.close()
+        e2e_s = time.perf_counter() - t0
     e2e_steps = int(st2["steps"])
     e2e_value = 6 * M * e2e_steps / e2e_s
     if dist:
@@ -308,14 +334,14 @@ def main():
     other = capi.PHI_PREC_FP64 if prec == capi.PHI_PREC_MIXED else capi.PHI_PREC_MIXED
     ho = Hierarchy(p, precision=other, device=local_rank)
     so = torch.cuda.ExternalStream(ho.stream_handle(), device=local_rank)
-    ho.rkf45_advance(DT0, T_END, TOL, MIN_DT, args.warmup)
+    run_steps(ho, args.warmup, True)
     torch.cuda.synchronize()
     e0o, e1o = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0o.record(so)
-    sto = ho.rkf45_advance(-1.0, T_END, TOL, MIN_DT, args.steps)
+    other_steps, _ = run_steps(ho, args.steps, False)
     e1o.record(so)
     e1o.synchronize()
-    other_ms_per_step = e0o.elapsed_time(e1o) / max(int(sto["steps"]), 1)
+    other_ms_per_step = e0o.elapsed_time(e1o) / max(other_steps, 1)
     ho.close()
     rho_full = {}
     for pr in (capi.PHI_PREC_FP64, capi.PHI_PREC_MIXED):
@@ -366,6 +392,7 @@ def main():
             "speedup_vs_fp64": (other_ms_per_step / ms_per_step) if other == capi.PHI_PREC_FP64 else
                                (ms_per_step / other_ms_per_step),
             "steps_timed": steps_done,
+            "propagations_completed_in_timed_region": propagations,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "heom_tile_kernel x6 + rkf45_control_kernel (one RKF45 step)",
@@ -374,8 +401,8 @@ def main():
                              "frac": apply_gbs / peak, "node_applies_per_s": M / (apply_ms / 1e3)},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / max(e2e_steps, 1),
                     "d2h_bytes_per_step": d2h / max(e2e_steps, 1),
-                    "what": "create (hierarchy built on device) + RKF45 + rho_0 read-back + destroy, "
-                            "host wall clock through the C ABI", "rho0_trace": float(np.trace(rho0).real)},
+                    "what": "create (hierarchy built on device) + full 1 ps RKF45 + rho_0 read-back + "
+                            "destroy, host wall clock through the C ABI (second of two runs)", "rho0_trace": float(np.trace(rho0).real)},
             "gpu_launches": ((steps_done + 15) // 16) * 16 * 7,
             "clocks": clocks,
         }

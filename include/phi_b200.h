@@ -183,6 +183,11 @@ PHI_API int phi_gpu_stream(const phi_ctx *ctx, void **stream);
 
 /* Time carried by the context (advanced by the integrators). */
 PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);
+/* Restores the initial hierarchy state (rho(0) in node 0, zeros elsewhere,
+ * InitializeDensityMatrix, hierarchy_integrator.cc:1070-1096) on the device,
+ * sets the time to `time` and forgets the RKF45 step size; no host transfer
+ * of the state. */
+PHI_API int phi_gpu_reset(phi_ctx *ctx, double time);
 PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);
 
 /* One RK4 step that allocates no memory, for callers that cannot call

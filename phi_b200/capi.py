@@ -102,6 +102,7 @@ SIGNATURES = [
     ("phi_gpu_stream", c_int, [c_void_p, POINTER(c_void_p)]),
     ("phi_gpu_get_time", c_int, [c_void_p, POINTER(c_double)]),
     ("phi_gpu_set_time", c_int, [c_void_p, c_double]),
+    ("phi_gpu_reset", c_int, [c_void_p, c_double]),
     ("phi_gpu_rk4_step_noalloc", c_int, [c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
 ]

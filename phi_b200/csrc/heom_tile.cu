@@ -183,7 +183,10 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
   double *coef = deph + NT;                                         // 24
-  int *ids = reinterpret_cast<int *>(coef + 24);                    // NT*2T
+  R *cn = reinterpret_cast<R *>(coef + 24);                          // NT*T |next prefactor|
+  R *cp = cn + NT * T;                                              // NT*T prev scale
+  R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
+  int *ids = reinterpret_cast<int *>(ccr + 2 * T);                  // NT*2T element offsets
   int *nts = ids + NT * 2 * T;                                      // NT*T
   unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
   unsigned char *pj = pi + P;
@@ -230,12 +233,25 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
     pi[i] = __ldg(c.pair_i + i);
     pj[i] = __ldg(c.pair_j + i);
   }
+  const int W = c.L + 2;
   const int tile_terms = nt_here * T;
+  // Per (node, term): neighbour ids scaled to element offsets of the stage
+  // input (-1 when absent), occupation, and the prefactor magnitudes for that
+  // occupation, so the pair loop reads shared memory only.
   for (int q = tid; q < tile_terms; q += 256) {
     const int nd = q / T, t = q - nd * T;
-    ids[nd * 2 * T + t] = __ldg(c.next + n0 * T + q);
-    ids[nd * 2 * T + T + t] = __ldg(c.prev + n0 * T + q);
-    nts[q] = __ldg(c.mi + n0 * T + q);
+    const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
+    const int nt = __ldg(c.mi + n0 * T + q);
+    ids[nd * 2 * T + t] = nx >= 0 ? nx * ES : -1;
+    ids[nd * 2 * T + T + t] = pv >= 0 ? pv * ES : -1;
+    nts[q] = nt;
+    cn[q] = (R)__ldg(c.sq_next + t * W + nt);
+    cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
+  }
+  for (int t = tid; t < T; t += 256) {
+    const double2 ct = __ldg(c.corr + t);
+    ccr[2 * t] = (R)ct.x;
+    ccr[2 * t + 1] = (R)ct.y;
   }
   __syncthreads();  // barrier init and metadata visible
   if (tid < nt_here) {
@@ -253,7 +269,6 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
 
   // ---- phase 2: derivative of every (node, pair) ----
   const R ih = (R)c.inv_hbar;
-  const int W = c.L + 2;
   const int items = nt_here * P;
   for (int it = tid; it < items; it += 256) {
     const int nd = it / P, u = it - nd * P;
@@ -281,7 +296,8 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
       vx = fma(-fac, xij.x, vx);
       vy = fma(-fac, xij.y, vy);
       const int *nid = ids + nd * 2 * T;
-      const int *nn = nts + nd * T;
+      const R *ncn = cn + nd * T, *ncp = cp + nd * T;
+      const int oij = i + j * N, oji = j + i * N;
       // Every neighbour value this pair needs, as independent predicated loads.
       TX gn_c[KT], gp_c[KT], gn_r[KT], gp_r[KT];
       const TX zero = mk<TX>(0.0, 0.0);
@@ -289,33 +305,31 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
       for (int q = 0; q < KT; ++q) {
         const int tj = j * KT + q, ti = i * KT + q;
         const int nxj = nid[tj], pvj = nid[T + tj], nxi = nid[ti], pvi = nid[T + ti];
-        gn_c[q] = (nxj >= 0 && i != j) ? __ldg(xin + (long long)nxj * ES + i + j * N) : zero;
-        gp_c[q] = (pvj >= 0 && i != j) ? __ldg(xin + (long long)pvj * ES + i + j * N) : zero;
-        gn_r[q] = (nxi >= 0 && i != j) ? __ldg(xin + (long long)nxi * ES + j + i * N) : zero;
-        gp_r[q] = pvi >= 0 ? __ldg(xin + (long long)pvi * ES + j + i * N) : zero;
+        gn_c[q] = (nxj >= 0 && i != j) ? __ldg(xin + nxj + oij) : zero;
+        gp_c[q] = (pvj >= 0 && i != j) ? __ldg(xin + pvj + oij) : zero;
+        gn_r[q] = (nxi >= 0 && i != j) ? __ldg(xin + nxi + oji) : zero;
+        gp_r[q] = pvi >= 0 ? __ldg(xin + pvi + oji) : zero;
       }
       if (i != j) {
 #pragma unroll
         for (int q = 0; q < KT; ++q) {
           const int tj = j * KT + q, ti = i * KT + q;
           // column part: + p X+_ij (p = i s), + i conj(c) sp X-_ij
-          const R sj = (R)__ldg(c.sq_next + tj * W + nn[tj]);
+          const R sj = ncn[tj];
           vx = fma(-sj, gn_c[q].y, vx);
           vy = fma(sj, gn_c[q].x, vy);
-          const R spj = (R)__ldg(c.sq_prev + tj * W + nn[tj]);
-          const double2 cjd = __ldg(c.corr + tj);
-          const R cjx = (R)cjd.x, cjy = (R)cjd.y;
+          const R spj = ncp[tj];
+          const R cjx = ccr[2 * tj], cjy = ccr[2 * tj + 1];
           const TX g = gp_c[q];
           const R re = cjx * g.x + cjy * g.y, im = cjx * g.y - cjy * g.x;
           vx = fma(-spj, im, vx);
           vy = fma(spj, re, vy);
           // row part: - p conj(X+_ji), - i c sp conj(X-_ji)
-          const R si = (R)__ldg(c.sq_next + ti * W + nn[ti]);
+          const R si = ncn[ti];
           vx = fma(-si, gn_r[q].y, vx);
           vy = fma(-si, gn_r[q].x, vy);
-          const R spi = (R)__ldg(c.sq_prev + ti * W + nn[ti]);
-          const double2 cid = __ldg(c.corr + ti);
-          const R cix = (R)cid.x, ciy = (R)cid.y;
+          const R spi = ncp[ti];
+          const R cix = ccr[2 * ti], ciy = ccr[2 * ti + 1];
           const TX h = gp_r[q];
           const R re2 = cix * h.x + ciy * h.y, im2 = ciy * h.x - cix * h.y;
           vx = fma(spi, im2, vx);
@@ -326,8 +340,8 @@ __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kerne
 #pragma unroll
         for (int q = 0; q < KT; ++q) {
           const int ti = i * KT + q;
-          const R spi = (R)__ldg(c.sq_prev + ti * W + nn[ti]);
-          const R ciy = (R)__ldg(c.corr + ti).y;
+          const R spi = ncp[ti];
+          const R ciy = ccr[2 * ti + 1];
           vx = fma((R)2 * spi * ciy, gp_r[q].x, vx);
         }
       }
@@ -452,6 +466,7 @@ size_t tile_smem(int T, int npre, const int *pre_bytes) {
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
   b += (size_t)(S::NT + 24) * sizeof(double);
+  b += (size_t)(2 * S::NT * T + 2 * T) * Lay::XB / 2;  // cn, cp, ccr in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;
   return b;
@@ -507,6 +522,8 @@ cudaError_t launch_tile_dispatch(const TileParams &p, cudaStream_t stream) {
 bool tile_kernel_available(const HeomConsts &c) {
   // IndependentBath with PHI's identity site map and K + 1 <= 3.
   if (c.kind != kIndependent || !c.identity_sites || c.K1 < 1 || c.K1 > 3 || c.nb != c.N) return false;
+  // neighbour offsets are 32-bit element indices of the stage input
+  if ((long long)c.M * (c.N * c.N + 1) >= (1ll << 31)) return false;
   switch (c.N) {
     case 2: case 3: case 4: case 5: case 6: case 7: case 8:
     case 10: case 12: case 16: case 24:

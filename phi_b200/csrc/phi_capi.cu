@@ -472,6 +472,17 @@ extern "C" int phi_gpu_get_time(const phi_ctx *ctx, double *time) {
   return PHI_OK;
 }
 
+extern "C" int phi_gpu_reset(phi_ctx *ctx, double time) {
+  if (!ctx) return PHI_E_INVALID;
+  const int N = ctx->desc.num_states;
+  PHI_CUDA(ctx, cudaMemsetAsync(ctx->y.ptr, 0, ctx->state_bytes(), ctx->stream));
+  PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
+                                cudaMemcpyHostToDevice, ctx->stream));
+  ctx->time = time;
+  ctx->rkf45_started = false;
+  return PHI_OK;
+}
+
 extern "C" int phi_gpu_set_time(phi_ctx *ctx, double time) {
   if (!ctx) return PHI_E_INVALID;
   ctx->time = time;

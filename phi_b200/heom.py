@@ -247,3 +247,7 @@ class Hierarchy:
         s = ctypes.c_void_p()
         self._check(self.lib.phi_gpu_stream(self.ctx, ctypes.byref(s)))
         return s.value or 0
+
+    def reset(self, time: float = 0.0) -> None:
+        """Initial state (rho(0) in node 0) restored on the device, time set."""
+        self._check(self.lib.phi_gpu_reset(self.ctx, float(time)))
