@@ -43,6 +43,8 @@ class PHI_API HierarchyIntegrator {
   phi_ctx *context() { return ctx_; }
   long long steps() const { return steps_; }
   long long accepted_steps() const { return accepted_; }
+  // Steady-state runs: BiCGSTAB iterations and final ||r||^2.
+  double residual() const { return residual_; }
 
  private:
   PhiParameters *parameters_;
@@ -51,12 +53,14 @@ class PHI_API HierarchyIntegrator {
   std::string error_;
   long long steps_ = 0;
   long long accepted_ = 0;
+  double residual_ = 0;
   bool has_result_ = false;
   Complex *result_ = nullptr;
 
   bool Prepare();
   void RunRk4(std::ofstream &out);
   void RunRkf45(std::ofstream &out);
+  void RunSteadyState(std::ofstream &out);
   void Fail(int code, const std::string &msg);
 };
 

@@ -181,6 +181,33 @@ PHI_API int phi_gpu_rkf45_advance(phi_ctx *ctx, double dt0, double t_end, double
  * own work or timing events after the library's. */
 PHI_API int phi_gpu_stream(const phi_ctx *ctx, void **stream);
 
+/* Stopping rules of phi_gpu_steady_state. */
+enum {
+  PHI_TOL_RELATIVE = 0,    /* ||r||_2 <= tol * ||b||_2 */
+  PHI_TOL_ABSOLUTE = 1,    /* ||r||_2 <= tol: BicgstabLSteadyState's diff
+                              (hierarchy_integrator.cc:3400-3421) */
+  PHI_TOL_ABS_SQUARED = 2  /* ||r||_2^2 <= tol: BicgstabSteadyState's diff
+                              (hierarchy_integrator.cc:3566-3594) on one thread */
+};
+
+/* Steady state of the hierarchy, L rho = 0 with tr rho_0 = 1, by
+ * BiCGSTAB(ell) on the device (replaces PrepForSteadyState followed by
+ * BicgstabLSteadyState / BicgstabSteadyState, hierarchy_integrator.cc:
+ * 1471-1613, :3112-3441, :3495-3783): rho_0[0,0] is eliminated, the
+ * right-hand side is minus the column of L that multiplies it, the equation
+ * of element (0,0) of node 0 is dropped and the solution is divided by
+ * tr rho_0.  ell in 1..8 (1 = BiCGSTAB; the reference's default is 2).
+ * Stops by tol_mode, or after max_steps BiCG steps (ell per outer iteration,
+ * the reference's `step`; 0 = 9999).  guess (host, 2*M*N*N doubles, may be
+ * NULL) is the initial hierarchy, scaled so that rho_0[0,0] = 1; NULL starts
+ * from rho_0 = I/N, other nodes 0 (the reference's guess without eigen
+ * data).  stats->iterations = BiCG steps taken; stats->residual = the
+ * quantity tol_mode compares with tol.  On return the context's state holds
+ * the last iterate, also when the solve stopped without converging
+ * (PHI_E_NO_CONVERGENCE).  FP64 in every precision. */
+PHI_API int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
+                                 const double *guess, phi_solve_stats *stats);
+
 /* Time carried by the context (advanced by the integrators). */
 PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);
 /* Restores the initial hierarchy state (rho(0) in node 0, zeros elsewhere,

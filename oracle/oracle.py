@@ -203,6 +203,59 @@ class Oracle:
     def rho0(self, state):
         return _from_colmajor(np.asarray(state)[:2 * self.n * self.n], self.n)
 
+    # -- steady state --------------------------------------------------------
+    # Coordinates of a Hermitian ADO X (N*N reals, in the column-major element
+    # order of the state): (i,i) -> Re X_ii, (i<j) -> Re X_ij, (i>j) -> Im X_ji.
+
+    def _to_coords(self, state):
+        n = self.n
+        z = np.asarray(state).view(np.complex128).reshape(self.M, n, n)  # z[m, j, i] = X_ij
+        x = np.transpose(z, (0, 2, 1))                                      # x[m, i, j] = X_ij
+        iu = np.triu_indices(n, 1)
+        c = np.empty((self.M, n, n))
+        c[:, np.arange(n), np.arange(n)] = x[:, np.arange(n), np.arange(n)].real
+        c[:, iu[0], iu[1]] = x[:, iu[0], iu[1]].real
+        c[:, iu[1], iu[0]] = x[:, iu[0], iu[1]].imag
+        return np.transpose(c, (0, 2, 1)).reshape(-1)                       # column-major like the state
+
+    def _from_coords(self, coords):
+        n = self.n
+        c = np.transpose(np.asarray(coords).reshape(self.M, n, n), (0, 2, 1))  # c[m, i, j]
+        iu = np.triu_indices(n, 1)
+        x = np.zeros((self.M, n, n), np.complex128)
+        x[:, np.arange(n), np.arange(n)] = c[:, np.arange(n), np.arange(n)]
+        upper = c[:, iu[0], iu[1]] + 1j * c[:, iu[1], iu[0]]
+        x[:, iu[0], iu[1]] = upper
+        x[:, iu[1], iu[0]] = np.conj(upper)
+        return np.ascontiguousarray(np.transpose(x, (0, 2, 1))).view(np.float64).reshape(-1)
+
+    def liouvillian_matrix(self):
+        """Real matrix of the Liouvillian on Hermitian hierarchies, in the
+        coordinates above (one oracle apply per basis element)."""
+        D = self.M * self.n * self.n
+        A = np.empty((D, D))
+        e = np.zeros(D)
+        for k in range(D):
+            e[k] = 1.0
+            A[:, k] = self._to_coords(self.apply(self._from_coords(e)))
+            e[k] = 0.0
+        return A
+
+    def steady_state(self, A=None):
+        """Steady state L rho = 0 by a dense solve of the system that
+        PrepForSteadyState / BicgstabSteadyState set up
+        (hierarchy_integrator.cc:1471-1613 and :3495-3513): rho_0[0,0] fixed to
+        1 and eliminated, minus its column of L as the right-hand side, the
+        equation of output element (0,0) of node 0 dropped (the zeroed top
+        row), and the solution divided by tr rho_0.  Small hierarchies only."""
+        if A is None:
+            A = self.liouvillian_matrix()
+        u = np.zeros(A.shape[0])
+        u[0] = 1.0
+        u[1:] = np.linalg.solve(A[1:, 1:], -A[1:, 0])
+        x = self._from_coords(u)
+        return x / np.trace(self.rho0(x)).real
+
 
 # ---------------------------------------------------------------------------
 # The reference itself (oracle/_ref/ref_driver), driven through PHI parameter

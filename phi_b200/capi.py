@@ -36,6 +36,9 @@ PHI_BATH_FULL = 2
 
 PHI_PREC_FP64 = 0
 PHI_PREC_MIXED = 1
+PHI_TOL_RELATIVE = 0
+PHI_TOL_ABSOLUTE = 1
+PHI_TOL_ABS_SQUARED = 2
 
 
 class PhiProblemDesc(ctypes.Structure):
@@ -100,6 +103,8 @@ SIGNATURES = [
     ("phi_gpu_rkf45_advance", c_int, [c_void_p, c_double, c_double, c_double, c_double, c_int64,
                                       POINTER(PhiRkf45Stats)]),
     ("phi_gpu_stream", c_int, [c_void_p, POINTER(c_void_p)]),
+    ("phi_gpu_steady_state", c_int, [c_void_p, c_int32, c_double, c_int32, c_int32, c_void_p,
+                                      POINTER(PhiSolveStats)]),
     ("phi_gpu_get_time", c_int, [c_void_p, POINTER(c_double)]),
     ("phi_gpu_set_time", c_int, [c_void_p, c_double]),
     ("phi_gpu_reset", c_int, [c_void_p, c_double]),

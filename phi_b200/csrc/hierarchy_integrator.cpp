@@ -4,6 +4,7 @@
 // closing lines).
 #include "../../include/phi/hierarchy_integrator.h"
 
+#include <algorithm>
 #include <cmath>
 #include <ctime>
 #include <fstream>
@@ -29,7 +30,8 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   if (p.filter_tolerance > 0) return reject("adaptive hierarchy filtering is outside this library's scope");
   if (p.is_restarted) return reject("restart input is outside this library's scope");
   if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
-  if (p.initial_density_matrix == nullptr)
+  const bool steady = p.run_method == BICGSTAB || p.run_method == BICGSTABL || p.run_method == BICGSTABU;
+  if (p.initial_density_matrix == nullptr && !steady)
     return reject("InitialDensityMatrix is required (the thermal guess needs LAPACK and is not supported)");
   if (p.gamma == nullptr || p.lambda == nullptr) return reject("Gamma and Lambda are required");
   *d = phi_problem_desc{};
@@ -45,6 +47,14 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   d->temperature = p.temperature;
   d->hamiltonian = reinterpret_cast<const double *>(p.time_indepenent_hamiltonian);
   d->initial_density_matrix = reinterpret_cast<const double *>(p.initial_density_matrix);
+  if (!d->initial_density_matrix) {
+    // Steady-state runs need no initial state; the context starts from I/N
+    // (copied by phi_gpu_create before this buffer is reused).
+    static thread_local std::vector<Complex> uniform;
+    uniform.assign((size_t)p.num_states * p.num_states, Complex(0, 0));
+    for (int i = 0; i < p.num_states; ++i) uniform[(size_t)i * (p.num_states + 1)] = 1.0 / p.num_states;
+    d->initial_density_matrix = reinterpret_cast<const double *>(uniform.data());
+  }
   d->gamma = p.gamma;
   d->lambda = p.lambda;
   d->coupling = (p.is_full_bath_coupling || p.is_diagonal_bath_coupling) ? p.bath_coupling_op : nullptr;
@@ -102,7 +112,8 @@ void HierarchyIntegrator::Launch() {
 }
 
 void HierarchyIntegrator::Run(int, int, RunMethod method) {
-  if (method != RK4 && method != RKF45) {
+  const bool steady = method == BICGSTAB || method == BICGSTABL || method == BICGSTABU;
+  if (method != RK4 && method != RKF45 && !steady) {
     Fail(PHI_E_INVALID, "run method not provided by this build of the library");
     return;
   }
@@ -118,15 +129,19 @@ void HierarchyIntegrator::Run(int, int, RunMethod method) {
     parameters_->Write(&out, M);
     out << "#Total Number of matrices:" << M << std::endl;
     out << "#Threads=" << parameters_->num_threads << "\n";
-    out << "#Integrator=" << (method == RK4 ? "rk4" : "rkf45") << "\n";
+    out << "#Integrator=" << (method == RK4 ? "rk4" : method == RKF45 ? "rkf45" : "bicgstab") << "\n";
     out << "#-------------\n";
-    out << parameters_->start_time << " ";
-    for (int i = 0; i < N * N; ++i) out << parameters_->initial_density_matrix[i] << " ";
-    out << "\n" << std::flush;
+    if (!steady) {
+      out << parameters_->start_time << " ";
+      for (int i = 0; i < N * N; ++i) out << parameters_->initial_density_matrix[i] << " ";
+      out << "\n";
+    }
+    out << std::flush;
   }
   if (method == RK4) RunRk4(out);
-  else RunRkf45(out);
-  if (status_ == PHI_OK) {
+  else if (method == RKF45) RunRkf45(out);
+  else RunSteadyState(out);
+  if (status_ == PHI_OK || (steady && status_ == PHI_E_NO_CONVERGENCE)) {
     delete[] result_;
     result_ = new Complex[(size_t)N * N];
     phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(result_));
@@ -216,6 +231,57 @@ void HierarchyIntegrator::RunRkf45(std::ofstream &out) {
   out << std::endl;
 }
 
+// BiCGSTAB(ell), BiCGSTAB and the "unstable" variant of the reference
+// (hierarchy_integrator.cc:3112, :3495, :3785) solve the same system.
+// BICGSTABL runs the device BiCGSTAB(ell) with ell = bicgstab_ell and the
+// reference's rule ||r|| <= BiCGSTABTolerance; BICGSTAB and BICGSTABU run
+// ell = 1 with ||r||^2 <= BiCGSTABTolerance and at most 9999 steps.  Output
+// follows :1595-1606 (initial guess) and :3730-3761 (closing lines and the
+// final rho_0 row).
+void HierarchyIntegrator::RunSteadyState(std::ofstream &out) {
+  const PhiParameters &p = *parameters_;
+  const int N = p.num_states;
+  if (out.is_open()) {
+    out << "#Initial rho:\n#";
+    for (int i = 0; i < N * N; ++i) out << Complex(i % (N + 1) == 0 ? 1.0 / N : 0.0, 0.0) << " ";
+    out << std::endl;
+  }
+  phi_solve_stats st{};
+  const std::time_t t1 = std::time(nullptr);
+  const bool ell_method = p.run_method == BICGSTABL;
+  const int ell = ell_method ? std::min(std::max(p.bicgstab_ell, 1), 8) : 1;
+  int rc = phi_gpu_steady_state(ctx_, ell, p.bicgstab_tolerance, ell_method ? PHI_TOL_ABSOLUTE : PHI_TOL_ABS_SQUARED,
+                                ell_method ? 999999 : 9999, nullptr, &st);
+  const std::time_t t2 = std::time(nullptr);
+  if (rc != PHI_OK && rc != PHI_E_NO_CONVERGENCE) {
+    char buf[512];
+    phi_gpu_last_error(ctx_, buf, sizeof buf);
+    Fail(rc, buf);
+    return;
+  }
+  steps_ = st.iterations;
+  accepted_ = st.iterations;
+  residual_ = st.residual;
+  if (rc == PHI_E_NO_CONVERGENCE) {
+    status_ = rc;
+    error_ = "BiCGSTAB did not converge";
+    if (p.verbose > -2) std::cout << "Convergence failed! (steps = " << st.iterations << ", diff = " << st.residual << ")\n";
+  } else if (p.verbose > -2) {
+    std::cout << "Converged to diff = " << st.residual << " in " << st.iterations << " steps.\n";
+  }
+  if (!out.is_open()) return;
+  if (rc == PHI_E_NO_CONVERGENCE)
+    out << "#Info: Total steps = " << st.iterations << ". No convergence.\n";
+  else
+    out << "#Info: Converged to diff = " << st.residual << " in " << st.iterations << " steps.\n";
+  out << "#Info: Total running time: " << std::difftime(t2, t1) / 60 / 60 / 24 << " days.\n";
+  std::vector<Complex> rho((size_t)N * N);
+  phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(rho.data()));
+  out << st.iterations << " ";
+  for (int j = 0; j < N * N; ++j) out << rho[j] << " ";
+  out << std::endl;
+}
+
 Complex *HierarchyIntegrator::density_matrix() {
   const int N = parameters_->num_states;
   Complex *rho = new Complex[(size_t)N * N];
@@ -241,6 +307,10 @@ extern "C" int phi_gpu_create_from_file(const char *path, const char *method, in
   std::cout.rdbuf(old);
   p.precision = precision;
   p.device = device;
+  if (p.run_method == NONE) {
+    phi::set_create_error("unknown integration method '" + ms + "'");
+    return PHI_E_INVALID;
+  }
   phi_problem_desc d;
   std::string err;
   int rc = phi::descriptor_from_parameters(p, &d, &err);

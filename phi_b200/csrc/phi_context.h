@@ -56,6 +56,14 @@ struct phi_ctx {
   cudaGraphExec_t rkf45_graph = nullptr;
   int rkf45_graph_steps = 0;
 
+  // Steady-state solve: x, rhat, b, r_0..r_ell, u_0..u_ell (complex128 state
+  // size each, one allocation) and the device scalar block; the captured
+  // graph replays outer iterations for bicg_ell.
+  phi::DeviceBuffer bicg_vecs;
+  phi::DeviceBuffer bicg_sc;
+  int bicg_ell = 0;
+  cudaGraphExec_t bicg_graph = nullptr;
+
   // RKF45 state kept between calls (phi_gpu_rkf45_advance with dt0 <= 0).
   phi::Rkf45Ctl rkf45_last{};
   bool rkf45_started = false;

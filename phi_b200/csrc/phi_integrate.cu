@@ -76,8 +76,10 @@ int phi_ctx::ensure_work(int level) {
 void phi_ctx::release_graphs() {
   if (rk4_graph) cudaGraphExecDestroy(rk4_graph);
   if (rkf45_graph) cudaGraphExecDestroy(rkf45_graph);
+  if (bicg_graph) cudaGraphExecDestroy(bicg_graph);
   rk4_graph = nullptr;
   rkf45_graph = nullptr;
+  bicg_graph = nullptr;
 }
 
 namespace {

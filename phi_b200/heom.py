@@ -140,12 +140,31 @@ class Hierarchy:
         ctx = ctypes.c_void_p()
         capi.check(self.lib.phi_gpu_create(ctypes.byref(d), ctypes.byref(ctx)))
         self.ctx = ctx
+        self._read_dims()
+
+    @classmethod
+    def from_file(cls, path: str, method: str = "rk4", precision: int = capi.PHI_PREC_FP64,
+                  device: int = 0) -> "Hierarchy":
+        """Context from a PHI parameter file (PhiParameters::ReadCommandLine,
+        phi_parameters.cc:93-146, then the library's scope checks)."""
+        self = cls.__new__(cls)
+        self.lib = capi.load()
+        self._keep = []
+        ctx = ctypes.c_void_p()
+        capi.check(self.lib.phi_gpu_create_from_file(str(path).encode(), method.encode(), precision, device,
+                                                     ctypes.byref(ctx)))
+        self.ctx = ctx
+        self._read_dims()
+        return self
+
+    def _read_dims(self):
         M = ctypes.c_int64()
         T = ctypes.c_int32()
         N = ctypes.c_int32()
         self._check(self.lib.phi_gpu_dims(self.ctx, ctypes.byref(M), ctypes.byref(T), ctypes.byref(N)))
         self.num_nodes = M.value
         self.num_terms = T.value
+        self.n = N.value
 
     def _check(self, code):
         capi.check(code, self.ctx)
@@ -251,3 +270,21 @@ class Hierarchy:
     def reset(self, time: float = 0.0) -> None:
         """Initial state (rho(0) in node 0) restored on the device, time set."""
         self._check(self.lib.phi_gpu_reset(self.ctx, float(time)))
+
+    def steady_state(self, tol: float = 1e-10, ell: int = 2, max_steps: int = 0, guess=None,
+                     tol_mode: int = capi.PHI_TOL_RELATIVE, check: bool = True):
+        """BiCGSTAB(ell) steady state (L rho = 0, tr rho_0 = 1); the context
+        state becomes the solution.  tol_mode: PHI_TOL_RELATIVE
+        (||r|| <= tol ||b||), PHI_TOL_ABSOLUTE (||r|| <= tol) or
+        PHI_TOL_ABS_SQUARED (||r||^2 <= tol)."""
+        st = capi.PhiSolveStats()
+        g = None
+        if guess is not None:
+            g = np.ascontiguousarray(guess, dtype=np.float64)
+            assert g.size == self.state_len
+        rc = self.lib.phi_gpu_steady_state(self.ctx, int(ell), float(tol), int(tol_mode), int(max_steps),
+                                           g.ctypes.data if g is not None else None, ctypes.byref(st))
+        if check:
+            self._check(rc)
+        return {"steps": st.iterations, "converged": bool(st.converged), "residual": st.residual,
+                "seconds": st.seconds, "status": rc}
