@@ -235,6 +235,50 @@ PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out
  * create when ctx is NULL) into buf. */
 PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
 
+/* ---- Batched instances ------------------------------------------------
+ * Many independent hierarchies of uneven N, K and depth integrated together
+ * (the reference runs one problem per process; this replaces a loop of
+ * HierarchyIntegrator::Launch over RK4 runs of many parameter sets,
+ * hierarchy_integrator.cc:113-175, :2593-2943).  Every RK4 stage of ALL
+ * instances runs as ONE persistent kernel launch over their concatenated
+ * tile lists; the step loop replays from a CUDA graph.  Each instance needs
+ * IndependentBath on PHI's identity site map, K + 1 <= 3 and N in
+ * {2..8, 10, 12, 16, 24}; all share one precision (desc.precision of the
+ * first) and one device.  Each instance's arithmetic is the one it gets
+ * alone in a phi_ctx. */
+typedef struct phi_batch phi_batch;
+
+typedef struct {
+  int32_t ctas_per_sm; /* persistent CTAs per SM (grid = ctas_per_sm * SMs) */
+  int32_t order;       /* 0: instances in the given order; 1: largest tiles first */
+  double ms_per_stage; /* measured by phi_gpu_batch_autotune (0 if not tuned) */
+} phi_batch_schedule;
+
+typedef struct {
+  int64_t steps;        /* RK4 steps taken by every instance */
+  int64_t node_applies; /* 4 * steps * sum of instance node counts */
+  double seconds;       /* device time of the steps (CUDA events) */
+  int64_t launches;     /* kernel launches issued for the steps */
+} phi_batch_stats;
+
+PHI_API int phi_gpu_batch_create(const phi_problem_desc *descs, int32_t count, phi_batch **out);
+PHI_API int phi_gpu_batch_destroy(phi_batch *batch);
+/* The context of instance `index` (owned by the batch): use it for dims,
+ * node tables, get/set state, rho_0 and time; do not integrate it while the
+ * batch is in use. */
+PHI_API int phi_gpu_batch_instance(phi_batch *batch, int32_t index, phi_ctx **ctx);
+/* Times the schedule candidates (CTAs per SM x work order) on one
+ * Liouvillian apply of every instance (state unchanged) and keeps the
+ * fastest for later RK4 calls; `chosen` may be NULL. */
+PHI_API int phi_gpu_batch_autotune(phi_batch *batch, phi_batch_schedule *chosen);
+PHI_API int phi_gpu_batch_set_schedule(phi_batch *batch, const phi_batch_schedule *schedule);
+/* `steps` RK4 steps of size dt on every instance (Rk4Integrate's stages,
+ * hierarchy_integrator.cc:2705-2826); each instance's time advances by
+ * repeated addition of dt, as in the reference's loop. */
+PHI_API int phi_gpu_batch_rk4(phi_batch *batch, double dt, int64_t steps, phi_batch_stats *stats);
+/* Last error of the batch (or of the last failed batch create when NULL). */
+PHI_API int phi_gpu_batch_last_error(const phi_batch *batch, char *buf, size_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,6 +84,23 @@ class PhiSolveStats(ctypes.Structure):
     ]
 
 
+class PhiBatchSchedule(ctypes.Structure):
+    _fields_ = [
+        ("ctas_per_sm", c_int32),
+        ("order", c_int32),
+        ("ms_per_stage", c_double),
+    ]
+
+
+class PhiBatchStats(ctypes.Structure):
+    _fields_ = [
+        ("steps", c_int64),
+        ("node_applies", c_int64),
+        ("seconds", c_double),
+        ("launches", c_int64),
+    ]
+
+
 # (name, restype, argtypes) for every entry point of include/phi_b200.h.
 SIGNATURES = [
     ("phi_gpu_create", c_int, [POINTER(PhiProblemDesc), POINTER(c_void_p)]),
@@ -110,6 +127,13 @@ SIGNATURES = [
     ("phi_gpu_reset", c_int, [c_void_p, c_double]),
     ("phi_gpu_rk4_step_noalloc", c_int, [c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
+    ("phi_gpu_batch_create", c_int, [POINTER(PhiProblemDesc), c_int32, POINTER(c_void_p)]),
+    ("phi_gpu_batch_destroy", c_int, [c_void_p]),
+    ("phi_gpu_batch_instance", c_int, [c_void_p, c_int32, POINTER(c_void_p)]),
+    ("phi_gpu_batch_autotune", c_int, [c_void_p, POINTER(PhiBatchSchedule)]),
+    ("phi_gpu_batch_set_schedule", c_int, [c_void_p, POINTER(PhiBatchSchedule)]),
+    ("phi_gpu_batch_rk4", c_int, [c_void_p, c_double, c_int64, POINTER(PhiBatchStats)]),
+    ("phi_gpu_batch_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
 ]
 
 _lib = None
@@ -151,3 +175,15 @@ def last_error(ctx=None) -> str:
 def check(code: int, ctx=None) -> None:
     if code != PHI_OK:
         raise PhiError(code, last_error(ctx))
+
+
+def batch_last_error(batch=None) -> str:
+    lib = load()
+    buf = ctypes.create_string_buffer(1024)
+    lib.phi_gpu_batch_last_error(batch, buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def check_batch(code: int, batch=None) -> None:
+    if code != PHI_OK:
+        raise PhiError(code, batch_last_error(batch))

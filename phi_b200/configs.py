@@ -106,3 +106,72 @@ def ring24(seed: int = 24, depth: int = 4) -> PhiParameters:
     p.seed = seed
     p.name = f"ring24_K0_L{depth}"
     return p
+
+
+BATCH_DIMS = (2, 3, 4, 6, 8, 12, 16)
+BATCH_BUDGET_BYTES = 256 * 2**20
+
+
+def hierarchy_nodes(terms: int, depth: int) -> int:
+    """Nodes of a hierarchy with `terms` exponentials truncated at tier
+    `depth`: C(terms + depth, depth)."""
+    from math import comb
+    return comb(terms + depth, depth)
+
+
+def batched(seed: int = 3, count: int = 512, budget_bytes: int = BATCH_BUDGET_BYTES,
+            depth_range=(4, 10)) -> list:
+    """Uneven independent instances: N uniform in {2,3,4,6,8,12,16}; a chain
+    with site energies U[0, 400] cm^-1 and nearest-neighbour couplings
+    N(0, 80 cm^-1); one Drude bath per site with lambda U[10, 100] cm^-1 and
+    1/gamma U[20, 200] fs; T U[77, 300] K; K in {0, 1}; depth L uniform in
+    depth_range.  Budget rule: while the FP64 state M*N^2*16 B exceeds
+    budget_bytes, L is decremented (floor 1); each instance records
+    `depth_drawn` and `depth`.  rho(0) = |0><0|; RK4 dt = 0.5 fs, 1000 steps.
+    N = 2 instances are dimers with one bath per site."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.choice(BATCH_DIMS))
+        k = int(rng.integers(0, 2))
+        depth = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        H = np.diag(rng.uniform(0.0, 400.0, size=n))
+        J = rng.normal(0.0, 80.0, size=n - 1)
+        for s in range(n - 1):
+            H[s, s + 1] = H[s + 1, s] = J[s]
+        lam = rng.uniform(10.0, 100.0, size=n)
+        tau_fs = rng.uniform(20.0, 200.0, size=n)
+        temp = float(rng.uniform(77.0, 300.0))
+        drawn = depth
+        terms = n * (k + 1)
+        while depth > 1 and hierarchy_nodes(terms, depth) * n * n * 16 > budget_bytes:
+            depth -= 1
+        p = PhiParameters(
+            num_states=n, time_indepenent_hamiltonian=H.astype(np.complex128),
+            num_bath_couplings=n, num_matsubara_terms=k + 1, hierarchy_truncation_level=depth + 1,
+            gamma=1000.0 / tau_fs, lambda_=lam,
+            initial_density_matrix=_basis_state(n, 0), temperature=temp,
+            timestep=0.0005, integration_time=0.5)
+        p.seed = seed
+        p.index = i
+        p.depth_drawn = drawn
+        p.depth = depth
+        p.nodes = hierarchy_nodes(terms, depth)
+        p.name = f"batch{seed}_{i}_N{n}_K{k}_L{depth}"
+        out.append(p)
+    return out
+
+
+def batch_summary(problems) -> dict:
+    """Histogram of effective depths, drawn-vs-effective depth changes and
+    the total FP64 state of a batched() draw."""
+    hist = {}
+    for p in problems:
+        hist[p.depth] = hist.get(p.depth, 0) + 1
+    return {
+        "instances": len(problems),
+        "depth_histogram": dict(sorted(hist.items())),
+        "depth_reduced": sum(1 for p in problems if p.depth != p.depth_drawn),
+        "total_nodes": int(sum(p.nodes for p in problems)),
+        "state_bytes_fp64": int(sum(p.nodes * p.num_states ** 2 * 16 for p in problems)),
+    }

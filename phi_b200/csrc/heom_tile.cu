@@ -1,475 +1,24 @@
-// heom_tile.cu -- tiled Liouvillian-apply / RK-stage kernel for the
-// IndependentBath model (PHI's default; hierarchy_updater.cc:129-144,
-// :216-254) with a compile-time system size N, in two arithmetics:
-//
-//   FP64   every buffer complex128 (the path PHI computes).
-//   MIXED  stage inputs X_s and stage derivatives k_s stored as complex64 and
-//          the Liouvillian evaluated in FP32; the state y, the RK4
-//          accumulator, every stage combine (X_{s+1} = y + sum b k), the
-//          fourth/fifth-order solutions, the RKF45 error norm and the step
-//          control stay FP64.  A complex64 copy of y (y32) is the stage-0
-//          input.  complex64 buffers pad every node to an even number of
-//          elements so each node range is 16-byte aligned.
-//
-// A 256-thread CTA owns a tile of NT consecutive nodes (about one
-// upper-triangle pair of one node per thread).  Everything the tile reads of
-// its own nodes is contiguous in HBM and arrives by TMA bulk copies issued at
-// CTA start:
-//
-//   t = 0   one thread issues cp.async.bulk copies of the tile's stage input
-//           X_s (barrier 0) and of every epilogue operand -- state y, RK4
-//           accumulator, RKF45 k_r -- (barrier 1) into shared memory; all
-//           threads load the tile's next/prev ids and occupations.
-//   phase 2 (after barrier 0) work item = (node, upper-triangle pair i <= j):
-//           A_ij, A_ji from shared memory (A = H X, [H, X] = A - A^+),
-//           dephasing + Matsubara factor, and the neighbour terms: for each
-//           term on site j (column part) or site i (row part), the one
-//           element of the linked ADO this pair needs, loaded from L2 with
-//           independent predicated loads (a Hermitian ADO's row m is the
-//           conjugate of its column m).  dX_ij and dX_ji = conj(dX_ij) go to
-//           shared memory.
-//   phase 3 (after barrier 1) epilogue per tile element: plain store, RK4 or
-//           RKF45 stage combine, RKF45 error max; operands from shared memory.
-//
-// Stores of the next stage input use the default cache policy (its neighbour
-// gathers in the next stage should hit L2); k and accumulator stores stream.
-// This kernel serves PHI's identity site map (bath m on |m><m|, terms of site
-// m are m*(K+1) .. m*(K+1)+K) with K+1 <= 3; other maps use the generic
-// kernel of heom_kernels.cu (FP64 only).
-//
-// Every mbarrier wait is bounded: after kMaxPolls polls the kernel records the
-// failure in HeomConsts::err_flag, waits (bounded again) for its own copies,
-// and returns; the host reports PHI_E_TIMEOUT.
+// heom_tile.cu -- tiled Liouvillian-apply / RK-stage kernel for one
+// IndependentBath hierarchy: one launch per stage over the hierarchy's tiles;
+// the tile itself is tile_body in heom_tile_body.cuh.
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <type_traits>
+#include <cstring>
 
-#include "heom_device.cuh"
-#include "heom_kernels.h"
-#include "heom_tile.h"
+#include "heom_tile_body.cuh"
 
 namespace phi {
+
+using namespace tile_detail;
+
 namespace {
 
-constexpr int kMaxPre = 5;  // epilogue operand buffers per launch
-constexpr long long kMaxPolls = 1ll << 22;
-
-struct TileParams {
-  HeomConsts c;
-  int mode;
-  int stage;
-  const void *x;        // stage input (TX)
-  void *out;            // apply output / next stage input (TX)
-  double2 *y;           // RK4 state
-  double2 *acc;         // RK4 accumulator
-  void *y32;            // MIXED RK4: complex64 copy of y (written at stage 3)
-  double a_next;
-  double w_acc;
-  Rk4Ctl *rk4;
-  double2 *traj;
-  void *k[5];           // RKF45 k0..k4 (TX)
-  double2 *ybuf[2];     // RKF45 state ping-pong
-  void *y32buf[2];      // MIXED RKF45: complex64 copies of ybuf
-  Rkf45Ctl *ctl;
-  int npre;                      // epilogue operands prefetched
-  const void *pre[kMaxPre];      // sources; slot 0 of RKF45 is chosen on the device
-  int pre_bytes[kMaxPre];        // 16 (complex128) or 8 (complex64)
-};
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-// One contiguous global -> shared copy (sizes and addresses multiples of 16 B).
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait on phase 0 of `bar`; false if it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar) {
-  for (long long i = 0; i < kMaxPolls; ++i)
-    if (mbar_try_wait(bar, 0)) return true;
-  return false;
-}
-
-// complex helpers over double2 / float2
-__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
-__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2(v.x, v.y); }
-template <class TX> __device__ __forceinline__ TX from_d2(double2 v);
-template <> __device__ __forceinline__ double2 from_d2<double2>(double2 v) { return v; }
-template <> __device__ __forceinline__ float2 from_d2<float2>(double2 v) {
-  return make_float2((float)v.x, (float)v.y);
-}
-template <class TX> __device__ __forceinline__ TX mk(double re, double im);
-template <> __device__ __forceinline__ double2 mk<double2>(double re, double im) { return make_double2(re, im); }
-template <> __device__ __forceinline__ float2 mk<float2>(double re, double im) {
-  return make_float2((float)re, (float)im);
-}
-__device__ __forceinline__ double2 cfma(double2 acc, double2 b, double s) {
-  return make_double2(fma(b.x, s, acc.x), fma(b.y, s, acc.y));
-}
-template <class TX> __device__ __forceinline__ void st_stream(TX *p, TX v) { __stcs(p, v); }
-
-template <int N>
-struct TileShape {
-  static constexpr int E = N * N;
-  static constexpr int EP = E + (E & 1);  // complex64 node stride (16-byte aligned nodes)
-  static constexpr int P = N * (N + 1) / 2;
-  static constexpr int NT0 = 256 / P;     // about one (node, pair) item per thread
-  static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
-};
-
-template <int N, bool MIXED>
-struct TileLayout {
-  using S = TileShape<N>;
-  static constexpr int ES = MIXED ? S::EP : S::E;  // node stride of X / k buffers
-  static constexpr int XB = MIXED ? 8 : 16;        // bytes per element of X / k
-  // byte offsets in dynamic shared memory
-  static constexpr size_t kBars = 0;
-  static constexpr size_t kX = 128;
-  static constexpr size_t kXBytes = ((size_t)S::NT * ES * XB + 127) / 128 * 128;
-  static constexpr size_t kU = kX + kXBytes;
-  static constexpr size_t kUBytes = ((size_t)S::NT * S::E * XB + 127) / 128 * 128;
-  static constexpr size_t kPre = kU + kUBytes;
-};
-
-// CTAs per SM the register budget is fitted to, without spills (ptxas -v):
-// more neighbour terms per site keep more gathered values live.
-template <int KT>
-struct TileMinBlocks {
-  static constexpr int value = KT == 1 ? 5 : (KT == 2 ? 4 : 3);
-};
-
-// KT = terms per site (K + 1) under PHI's identity site map.
 template <int N, int KT, bool MIXED>
 __global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kernel(TileParams p) {
-  using S = TileShape<N>;
-  using Lay = TileLayout<N, MIXED>;
-  using TX = typename std::conditional<MIXED, float2, double2>::type;
-  using R = typename std::conditional<MIXED, float, double>::type;
-  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const HeomConsts &c = p.c;
-  const int T = c.T;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Lay::kBars);
-  TX *Xs = reinterpret_cast<TX *>(smem_raw + Lay::kX);   // NT*ES
-  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*E
-  unsigned char *PreBase = smem_raw + Lay::kPre;
-  size_t pre_off[kMaxPre];
-  size_t tail = Lay::kPre;
-  for (int b = 0; b < kMaxPre; ++b) {
-    pre_off[b] = tail - Lay::kPre;
-    if (b < p.npre) tail += ((size_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
-  }
-  TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
-  double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
-  double *coef = deph + NT;                                         // 24
-  R *cn = reinterpret_cast<R *>(coef + 24);                          // NT*T |next prefactor|
-  R *cp = cn + NT * T;                                              // NT*T prev scale
-  R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
-  int *ids = reinterpret_cast<int *>(ccr + 2 * T);                  // NT*2T element offsets
-  int *nts = ids + NT * 2 * T;                                      // NT*T
-  unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
-  unsigned char *pj = pi + P;
-
-  const int tid = threadIdx.x;
-  int ycur = 0;
-  if (p.mode == kModeRkf45) {
-    if (*(volatile int *)&p.ctl->done) return;  // uniform across the grid
-    ycur = p.ctl->ycur;
-    if (tid < 24) coef[tid] = p.ctl->coef[tid];
-  }
-  const long long n0 = (long long)blockIdx.x * NT;
-  if (n0 >= c.M) return;
-  const int nt_here = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
-  const TX *xin;
-  if (p.mode == kModeRkf45 && p.stage == 0)
-    xin = MIXED ? static_cast<const TX *>(p.y32buf[ycur]) : reinterpret_cast<const TX *>(p.ybuf[ycur]);
-  else
-    xin = static_cast<const TX *>(p.x);
-  const int tile_elems = nt_here * E;
-
-  // ---- t = 0: bulk prefetch of the tile's contiguous ranges ----
-  if (tid == 0) {
-    mbar_init(&bars[0], 1);
-    mbar_init(&bars[1], 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    const uint32_t xbytes = (uint32_t)(nt_here * ES * Lay::XB);
-    mbar_expect_tx(&bars[0], xbytes);
-    bulk_g2s(Xs, xin + n0 * ES, xbytes, &bars[0]);
-    uint32_t pbytes = 0;
-    for (int b = 0; b < p.npre; ++b)
-      pbytes += (uint32_t)(nt_here * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
-    mbar_expect_tx(&bars[1], pbytes);
-    for (int b = 0; b < p.npre; ++b) {
-      const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
-      if (b == 0 && p.mode == kModeRkf45) src = reinterpret_cast<const unsigned char *>(p.ybuf[ycur]);
-      const int stride = p.pre_bytes[b] == 16 ? E : ES;
-      const uint32_t bytes = (uint32_t)(nt_here * stride * p.pre_bytes[b]);
-      bulk_g2s(PreBase + pre_off[b], src + (size_t)n0 * stride * p.pre_bytes[b], bytes, &bars[1]);
-    }
-  }
-  for (int i = tid; i < E; i += 256) Hs[i] = from_d2<TX>(__ldg(c.H + i));
-  for (int i = tid; i < P; i += 256) {
-    pi[i] = __ldg(c.pair_i + i);
-    pj[i] = __ldg(c.pair_j + i);
-  }
-  const int W = c.L + 2;
-  const int tile_terms = nt_here * T;
-  // Per (node, term): neighbour ids scaled to element offsets of the stage
-  // input (-1 when absent), occupation, and the prefactor magnitudes for that
-  // occupation, so the pair loop reads shared memory only.
-  for (int q = tid; q < tile_terms; q += 256) {
-    const int nd = q / T, t = q - nd * T;
-    const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
-    const int nt = __ldg(c.mi + n0 * T + q);
-    ids[nd * 2 * T + t] = nx >= 0 ? nx * ES : -1;
-    ids[nd * 2 * T + T + t] = pv >= 0 ? pv * ES : -1;
-    nts[q] = nt;
-    cn[q] = (R)__ldg(c.sq_next + t * W + nt);
-    cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
-  }
-  for (int t = tid; t < T; t += 256) {
-    const double2 ct = __ldg(c.corr + t);
-    ccr[2 * t] = (R)ct.x;
-    ccr[2 * t + 1] = (R)ct.y;
-  }
-  __syncthreads();  // barrier init and metadata visible
-  if (tid < nt_here) {
-    double d = 0.0;
-    for (int t = 0; t < T; ++t) d += nts[tid * T + t] * __ldg(c.nu + t);
-    deph[tid] = d;
-  }
-  bool ok = mbar_wait_bounded(&bars[0]);
-  __syncthreads();  // deph visible
-  if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicOr(c.err_flag, 1);
-    mbar_wait_bounded(&bars[1]);
-    return;
-  }
-
-  // ---- phase 2: derivative of every (node, pair) ----
-  const R ih = (R)c.inv_hbar;
-  const int items = nt_here * P;
-  for (int it = tid; it < items; it += 256) {
-    const int nd = it / P, u = it - nd * P;
-    const int i = pi[u], j = pj[u];
-    const TX *X = Xs + nd * ES;
-    R ar = 0, ai = 0, br = 0, bi = 0;  // A_ij, A_ji
-#pragma unroll
-    for (int k = 0; k < N; ++k) {
-      const TX hik = Hs[i + k * N], xkj = X[k + j * N];
-      const TX hjk = Hs[j + k * N], xki = X[k + i * N];
-      ar = fma(hik.x, xkj.x, ar);
-      ar = fma(-hik.y, xkj.y, ar);
-      ai = fma(hik.x, xkj.y, ai);
-      ai = fma(hik.y, xkj.x, ai);
-      br = fma(hjk.x, xki.x, br);
-      br = fma(-hjk.y, xki.y, br);
-      bi = fma(hjk.x, xki.y, bi);
-      bi = fma(hjk.y, xki.x, bi);
-    }
-    // -i/hbar (A_ij - conj(A_ji))
-    R vx = (ai + bi) * ih, vy = -(ar - br) * ih;
-    const TX xij = X[i + j * N];
-    if (!c.vacuum) {
-      const R fac = (R)(deph[nd] + __ldg(c.mats_elem + i + j * N));
-      vx = fma(-fac, xij.x, vx);
-      vy = fma(-fac, xij.y, vy);
-      const int *nid = ids + nd * 2 * T;
-      const R *ncn = cn + nd * T, *ncp = cp + nd * T;
-      const int oij = i + j * N, oji = j + i * N;
-      // Every neighbour value this pair needs, as independent predicated loads.
-      TX gn_c[KT], gp_c[KT], gn_r[KT], gp_r[KT];
-      const TX zero = mk<TX>(0.0, 0.0);
-#pragma unroll
-      for (int q = 0; q < KT; ++q) {
-        const int tj = j * KT + q, ti = i * KT + q;
-        const int nxj = nid[tj], pvj = nid[T + tj], nxi = nid[ti], pvi = nid[T + ti];
-        gn_c[q] = (nxj >= 0 && i != j) ? __ldg(xin + nxj + oij) : zero;
-        gp_c[q] = (pvj >= 0 && i != j) ? __ldg(xin + pvj + oij) : zero;
-        gn_r[q] = (nxi >= 0 && i != j) ? __ldg(xin + nxi + oji) : zero;
-        gp_r[q] = pvi >= 0 ? __ldg(xin + pvi + oji) : zero;
-      }
-      if (i != j) {
-#pragma unroll
-        for (int q = 0; q < KT; ++q) {
-          const int tj = j * KT + q, ti = i * KT + q;
-          // column part: + p X+_ij (p = i s), + i conj(c) sp X-_ij
-          const R sj = ncn[tj];
-          vx = fma(-sj, gn_c[q].y, vx);
-          vy = fma(sj, gn_c[q].x, vy);
-          const R spj = ncp[tj];
-          const R cjx = ccr[2 * tj], cjy = ccr[2 * tj + 1];
-          const TX g = gp_c[q];
-          const R re = cjx * g.x + cjy * g.y, im = cjx * g.y - cjy * g.x;
-          vx = fma(-spj, im, vx);
-          vy = fma(spj, re, vy);
-          // row part: - p conj(X+_ji), - i c sp conj(X-_ji)
-          const R si = ncn[ti];
-          vx = fma(-si, gn_r[q].y, vx);
-          vy = fma(-si, gn_r[q].x, vy);
-          const R spi = ncp[ti];
-          const R cix = ccr[2 * ti], ciy = ccr[2 * ti + 1];
-          const TX h = gp_r[q];
-          const R re2 = cix * h.x + ciy * h.y, im2 = ciy * h.x - cix * h.y;
-          vx = fma(spi, im2, vx);
-          vy = fma(-spi, re2, vy);
-        }
-      } else {
-        // diagonal: next terms cancel; prev gives 2 sp Im(c) X-_mm
-#pragma unroll
-        for (int q = 0; q < KT; ++q) {
-          const int ti = i * KT + q;
-          const R spi = ncp[ti];
-          const R ciy = ccr[2 * ti + 1];
-          vx = fma((R)2 * spi * ciy, gp_r[q].x, vx);
-        }
-      }
-    }
-    TX v;
-    v.x = vx;
-    v.y = vy;
-    if (i == j) {
-      v.y = 0;
-      Us[nd * E + i + j * N] = v;
-    } else {
-      Us[nd * E + i + j * N] = v;
-      v.y = -v.y;
-      Us[nd * E + j + i * N] = v;
-    }
-  }
-  ok = p.npre == 0 || mbar_wait_bounded(&bars[1]);
-  if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicOr(c.err_flag, 1);
-    return;
-  }
-
-  // ---- phase 3: epilogue over the tile's elements ----
-  // element e of the tile: node nd = e / E, offset w = e % E; complex128
-  // buffers are indexed (n0 + nd) * E + w, X / k buffers (n0 + nd) * ES + w.
-  auto preD = [&](int b) { return reinterpret_cast<const double2 *>(PreBase + pre_off[b]); };
-  auto preX = [&](int b) { return reinterpret_cast<const TX *>(PreBase + pre_off[b]); };
-  double emax = 0.0;
-  if (p.mode == kModeApply) {
-    TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += 256) {
-      const int nd = e / E, w = e - nd * E;
-      st_stream(out + (n0 + nd) * ES + w, Us[e]);
-    }
-  } else if (p.mode == kModeRk4) {
-    const int s = p.stage;
-    TX *out = static_cast<TX *>(p.out);
-    long long row = -1;
-    if (s == 3 && n0 == 0 && p.traj) {
-      const Rk4Ctl *rc = p.rk4;
-      if (rc->out_factor > 0 && rc->step % rc->out_factor == 0 && rc->nout < rc->capacity) row = rc->nout;
-    }
-    for (int e = tid; e < tile_elems; e += 256) {
-      const int nd = e / E, w = e - nd * E;
-      const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
-      const double2 kv = to_d2(Us[e]);
-      if (s == 0) {  // FP64: pre = {} (y is the input); MIXED: pre = {y}
-        const double2 ys = MIXED ? preD(0)[e] : to_d2(Xs[nd * ES + w]);
-        out[gx] = from_d2<TX>(cfma(ys, kv, p.a_next));
-        st_stream(p.acc + gd, cfma(ys, kv, p.w_acc));
-      } else if (s < 3) {  // pre = {y, acc}
-        out[gx] = from_d2<TX>(cfma(preD(0)[e], kv, p.a_next));
-        st_stream(p.acc + gd, cfma(preD(1)[e], kv, p.w_acc));
-      } else {             // pre = {acc}
-        const double2 yn = cfma(preD(0)[e], kv, p.w_acc);
-        p.y[gd] = yn;
-        if (MIXED) static_cast<TX *>(p.y32)[gx] = from_d2<TX>(yn);
-        if (row >= 0 && e < E) p.traj[row * E + e] = yn;
-      }
-    }
-    if (s == 3 && n0 == 0 && p.traj) {
-      __syncthreads();
-      if (tid == 0) {
-        Rk4Ctl *rc = p.rk4;
-        if (row >= 0) rc->nout = rc->nout + 1;
-        rc->step = rc->step + 1;
-      }
-    }
-  } else {
-    const int s = p.stage;
-    const double *cf = coef;
-    TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += 256) {
-      const int nd = e / E, w = e - nd * E;
-      const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
-      const TX kx = Us[e];
-      const double2 kv = to_d2(kx);
-      if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; FP64 stage 0: y is the input
-        const double2 ys = (s == 0 && !MIXED) ? to_d2(Xs[nd * ES + w]) : preD(0)[e];
-        st_stream(static_cast<TX *>(p.k[s]) + gx, kx);
-        const int row = s * (s + 1) / 2;
-        double2 xv = ys;
-        for (int r = 0; r < s; ++r) xv = cfma(xv, to_d2(preX(1 + r)[nd * ES + w]), cf[row + r]);
-        xv = cfma(xv, kv, cf[row + s]);
-        out[gx] = from_d2<TX>(xv);
-      } else {      // pre = {y, k0, k2, k3, k4}
-        const double2 ys = preD(0)[e];
-        const double2 k0 = to_d2(preX(1)[nd * ES + w]), k2 = to_d2(preX(2)[nd * ES + w]);
-        const double2 k3 = to_d2(preX(3)[nd * ES + w]), k4 = to_d2(preX(4)[nd * ES + w]);
-        double2 y4 = cfma(ys, k0, cf[15]);
-        y4 = cfma(y4, k2, cf[16]);
-        y4 = cfma(y4, k3, cf[17]);
-        y4 = cfma(y4, k4, cf[18]);
-        double2 y5 = cfma(ys, k0, cf[19]);
-        y5 = cfma(y5, k2, cf[20]);
-        y5 = cfma(y5, k3, cf[21]);
-        y5 = cfma(y5, k4, cf[22]);
-        y5 = cfma(y5, kv, cf[23]);
-        st_stream(p.ybuf[ycur ^ 1] + gd, y5);
-        if (MIXED) st_stream(static_cast<TX *>(p.y32buf[ycur ^ 1]) + gx, from_d2<TX>(y5));
-        const double err = hypot(y4.x - y5.x, y4.y - y5.y);
-        emax = (err > emax || err != err) ? err : emax;
-      }
-    }
-    if (s == 5) {
-      unsigned long long bits = (unsigned long long)__double_as_longlong(emax);
-      for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
-        bits = o > bits ? o : bits;
-      }
-      if ((tid & 31) == 0 && bits) atomicMax(&p.ctl->err_bits, bits);
-    }
-  }
-}
-
-template <int N, bool MIXED>
-size_t tile_smem(int T, int npre, const int *pre_bytes) {
-  using S = TileShape<N>;
-  using Lay = TileLayout<N, MIXED>;
-  size_t b = Lay::kPre;
-  for (int i = 0; i < npre; ++i)
-    b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
-  b += (size_t)S::E * Lay::XB;
-  b += (size_t)(S::NT + 24) * sizeof(double);
-  b += (size_t)(2 * S::NT * T + 2 * T) * Lay::XB / 2;  // cn, cp, ccr in the arithmetic type
-  b += (size_t)(S::NT * 3 * T) * sizeof(int);
-  b += 2 * S::P + 16;
-  return b;
+  tile_init_barriers(smem_raw);
+  tile_body<N, KT, MIXED>(p, blockIdx.x, smem_raw, 0u, 0u);
 }
 
 template <int N, int KT, bool MIXED>
@@ -535,7 +84,8 @@ bool tile_kernel_available(const HeomConsts &c) {
 
 int mixed_node_stride(int N) { return N * N + ((N * N) & 1); }
 
-cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
+namespace tile_detail {
+TileParams tile_params_for(const StageLaunch &L) {
   TileParams p;
   p.c = L.c;
   p.mode = L.mode;
@@ -593,7 +143,67 @@ cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
       }
     }
   }
-  return mixed ? launch_tile_dispatch<true>(p, stream) : launch_tile_dispatch<false>(p, stream);
+  return p;
 }
+}  // namespace tile_detail
+
+cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
+  const TileParams p = tile_params_for(L);
+  return L.mixed ? launch_tile_dispatch<true>(p, stream) : launch_tile_dispatch<false>(p, stream);
+}
+
+namespace {
+template <int N>
+long long tiles_of(long long M) {
+  return (M + TileShape<N>::NT - 1) / TileShape<N>::NT;
+}
+template <int N>
+size_t stage_smem_n(const TileParams &p, bool mixed) {
+  return mixed ? tile_smem<N, true>(p.c.T, p.npre, p.pre_bytes) : tile_smem<N, false>(p.c.T, p.npre, p.pre_bytes);
+}
+}  // namespace
+
+long long tile_count(const HeomConsts &c) {
+  switch (c.N) {
+    case 2: return tiles_of<2>(c.M);
+    case 3: return tiles_of<3>(c.M);
+    case 4: return tiles_of<4>(c.M);
+    case 5: return tiles_of<5>(c.M);
+    case 6: return tiles_of<6>(c.M);
+    case 7: return tiles_of<7>(c.M);
+    case 8: return tiles_of<8>(c.M);
+    case 10: return tiles_of<10>(c.M);
+    case 12: return tiles_of<12>(c.M);
+    case 16: return tiles_of<16>(c.M);
+    case 24: return tiles_of<24>(c.M);
+    default: return -1;
+  }
+}
+
+size_t tile_stage_smem(const StageLaunch &L) {
+  const TileParams p = tile_params_for(L);
+  switch (L.c.N) {
+    case 2: return stage_smem_n<2>(p, L.mixed);
+    case 3: return stage_smem_n<3>(p, L.mixed);
+    case 4: return stage_smem_n<4>(p, L.mixed);
+    case 5: return stage_smem_n<5>(p, L.mixed);
+    case 6: return stage_smem_n<6>(p, L.mixed);
+    case 7: return stage_smem_n<7>(p, L.mixed);
+    case 8: return stage_smem_n<8>(p, L.mixed);
+    case 10: return stage_smem_n<10>(p, L.mixed);
+    case 12: return stage_smem_n<12>(p, L.mixed);
+    case 16: return stage_smem_n<16>(p, L.mixed);
+    case 24: return stage_smem_n<24>(p, L.mixed);
+    default: return 0;
+  }
+}
+
+size_t tile_params_bytes() { return sizeof(TileParams); }
+
+void tile_params_host(const StageLaunch &L, void *out) {
+  const TileParams p = tile_params_for(L);
+  std::memcpy(out, &p, sizeof(p));
+}
+
 
 }  // namespace phi

@@ -96,51 +96,70 @@ def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+def problem_desc(p: PhiParameters, precision: int, device: int, max_nodes: int, keep_list: list):
+    """phi_problem_desc of a PhiParameters; the arrays it points to are
+    appended to keep_list (the caller keeps them alive)."""
+    n = int(p.num_states)
+    d = capi.PhiProblemDesc()
+    d.num_states = n
+    d.num_baths = int(p.num_bath_couplings)
+    d.num_matsubara_terms = int(p.num_matsubara_terms)
+    d.truncation_level = int(p.hierarchy_truncation_level)
+    d.bath_kind = p.bath_kind
+    d.normalized = 1 if p.is_rho_normalized else 0
+    d.hbar = float(p.hbar)
+    d.boltzmann_constant = float(p.boltzmann_constant)
+    d.temperature = float(p.temperature)
+
+    def keep(a, dtype=np.float64):
+        a = np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1))
+        keep_list.append(a)
+        return a
+
+    d.hamiltonian = _dptr(keep(col_major(p.time_indepenent_hamiltonian)))
+    d.initial_density_matrix = _dptr(keep(col_major(p.initial_density_matrix)))
+    d.gamma = _dptr(keep(p.gamma))
+    d.lambda_ = _dptr(keep(p.lambda_))
+    if p.bath_coupling_op is not None and p.bath_kind != capi.PHI_BATH_INDEPENDENT:
+        v = np.asarray(p.bath_coupling_op, dtype=np.float64)
+        if p.bath_kind == capi.PHI_BATH_FULL:
+            # (nb, N, N) [row, col] -> per-bath column-major
+            v = np.ascontiguousarray(np.transpose(v.reshape(-1, n, n), (0, 2, 1)))
+        d.coupling = _dptr(keep(v))
+    if p.bath_sites is not None:
+        s = keep(p.bath_sites, np.int32)
+        d.bath_sites = s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+    d.precision = precision
+    d.device = device
+    d.max_nodes = max_nodes
+    return d
+
+
 class Hierarchy:
     """One hierarchy instance on one GPU (a phi_ctx)."""
 
     def __init__(self, p: PhiParameters, precision: int = capi.PHI_PREC_FP64,
                  device: int = 0, max_nodes: int = 0):
         self.lib = capi.load()
-        n = int(p.num_states)
-        self.n = n
+        self.n = int(p.num_states)
         self._keep = []
-        d = capi.PhiProblemDesc()
-        d.num_states = n
-        d.num_baths = int(p.num_bath_couplings)
-        d.num_matsubara_terms = int(p.num_matsubara_terms)
-        d.truncation_level = int(p.hierarchy_truncation_level)
-        d.bath_kind = p.bath_kind
-        d.normalized = 1 if p.is_rho_normalized else 0
-        d.hbar = float(p.hbar)
-        d.boltzmann_constant = float(p.boltzmann_constant)
-        d.temperature = float(p.temperature)
-
-        def keep(a, dtype=np.float64):
-            a = np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1))
-            self._keep.append(a)
-            return a
-
-        d.hamiltonian = _dptr(keep(col_major(p.time_indepenent_hamiltonian)))
-        d.initial_density_matrix = _dptr(keep(col_major(p.initial_density_matrix)))
-        d.gamma = _dptr(keep(p.gamma))
-        d.lambda_ = _dptr(keep(p.lambda_))
-        if p.bath_coupling_op is not None and p.bath_kind != capi.PHI_BATH_INDEPENDENT:
-            v = np.asarray(p.bath_coupling_op, dtype=np.float64)
-            if p.bath_kind == capi.PHI_BATH_FULL:
-                # (nb, N, N) [row, col] -> per-bath column-major
-                v = np.ascontiguousarray(np.transpose(v.reshape(-1, n, n), (0, 2, 1)))
-            d.coupling = _dptr(keep(v))
-        if p.bath_sites is not None:
-            s = keep(p.bath_sites, np.int32)
-            d.bath_sites = s.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
-        d.precision = precision
-        d.device = device
-        d.max_nodes = max_nodes
+        d = problem_desc(p, precision, device, max_nodes, self._keep)
         ctx = ctypes.c_void_p()
         capi.check(self.lib.phi_gpu_create(ctypes.byref(d), ctypes.byref(ctx)))
         self.ctx = ctx
         self._read_dims()
+
+    @classmethod
+    def _borrowed(cls, lib, ctx) -> "Hierarchy":
+        """View of a context owned elsewhere (a batch instance); close() does
+        not destroy it."""
+        self = cls.__new__(cls)
+        self.lib = lib
+        self._keep = []
+        self.ctx = ctx
+        self._owned = False
+        self._read_dims()
+        return self
 
     @classmethod
     def from_file(cls, path: str, method: str = "rk4", precision: int = capi.PHI_PREC_FP64,
@@ -171,7 +190,8 @@ class Hierarchy:
 
     def close(self):
         if getattr(self, "ctx", None):
-            self.lib.phi_gpu_destroy(self.ctx)
+            if getattr(self, "_owned", True):
+                self.lib.phi_gpu_destroy(self.ctx)
             self.ctx = None
 
     def __del__(self):
@@ -288,3 +308,68 @@ class Hierarchy:
             self._check(rc)
         return {"steps": st.iterations, "converged": bool(st.converged), "residual": st.residual,
                 "seconds": st.seconds, "status": rc}
+
+
+class Batch:
+    """Many independent hierarchies integrated together (a phi_batch): every
+    RK4 stage of all instances is one persistent kernel launch."""
+
+    def __init__(self, problems, precision: int = capi.PHI_PREC_FP64, device: int = 0):
+        self.lib = capi.load()
+        self._keep = []
+        arr = (capi.PhiProblemDesc * len(problems))()
+        for i, p in enumerate(problems):
+            arr[i] = problem_desc(p, precision, device, 0, self._keep)
+        b = ctypes.c_void_p()
+        capi.check_batch(self.lib.phi_gpu_batch_create(arr, len(problems), ctypes.byref(b)))
+        self.batch = b
+        self.count = len(problems)
+        self.instances = []
+        for i in range(self.count):
+            c = ctypes.c_void_p()
+            self._check(self.lib.phi_gpu_batch_instance(self.batch, i, ctypes.byref(c)))
+            self.instances.append(Hierarchy._borrowed(self.lib, c))
+
+    def _check(self, code):
+        capi.check_batch(code, self.batch)
+
+    def close(self):
+        if getattr(self, "batch", None):
+            for h in self.instances:
+                h.close()
+            self.lib.phi_gpu_batch_destroy(self.batch)
+            self.batch = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __getitem__(self, i) -> Hierarchy:
+        return self.instances[i]
+
+    @property
+    def total_nodes(self) -> int:
+        return sum(h.num_nodes for h in self.instances)
+
+    def autotune(self) -> dict:
+        s = capi.PhiBatchSchedule()
+        self._check(self.lib.phi_gpu_batch_autotune(self.batch, ctypes.byref(s)))
+        return {"ctas_per_sm": s.ctas_per_sm, "order": s.order, "ms_per_stage": s.ms_per_stage}
+
+    def set_schedule(self, ctas_per_sm: int, order: int):
+        s = capi.PhiBatchSchedule(ctas_per_sm, order, 0.0)
+        self._check(self.lib.phi_gpu_batch_set_schedule(self.batch, ctypes.byref(s)))
+
+    def rk4(self, dt: float, steps: int) -> dict:
+        st = capi.PhiBatchStats()
+        self._check(self.lib.phi_gpu_batch_rk4(self.batch, float(dt), int(steps), ctypes.byref(st)))
+        return {"steps": st.steps, "node_applies": st.node_applies, "seconds": st.seconds,
+                "launches": st.launches}
