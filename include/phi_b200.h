@@ -279,6 +279,34 @@ PHI_API int phi_gpu_batch_rk4(phi_batch *batch, double dt, int64_t steps, phi_ba
 /* Last error of the batch (or of the last failed batch create when NULL). */
 PHI_API int phi_gpu_batch_last_error(const phi_batch *batch, char *buf, size_t len);
 
+/* ---- Learned initial guess for the steady state ------------------------
+ * Kernels of the small multilayer perceptron that maps a problem's
+ * parameters to its steady-state rho_0 (the initial guess of
+ * phi_gpu_steady_state_rho0).  All pointers are device pointers; `stream` is
+ * a cudaStream_t (NULL = default stream).  Layer: Y = act(X W^T + b),
+ * X: B x in FP32 row-major, W: out x in BF16 row-major, b: FP32; act 1 =
+ * tanh, 0 = identity; FP32 accumulation. */
+PHI_API int phi_nn_linear_forward(const float *X, const void *W_bf16, const float *b, float *Y, int32_t B,
+                                  int32_t in, int32_t out, int32_t act, void *stream);
+/* Backward of one layer given dY (overwritten with dZ = dY * act'(Y)):
+ * dW = dZ^T X, db = column sums of dZ, dX = dZ W (skipped when dX is NULL). */
+PHI_API int phi_nn_linear_backward(float *dY, const float *Y, const float *X, const void *W_bf16, float *dX,
+                                   float *dW, float *db, int32_t B, int32_t in, int32_t out, int32_t act,
+                                   void *stream);
+/* loss = sum (P - T)^2 / B over n = B * width values; dP = 2 (P - T) / B. */
+PHI_API int phi_nn_mse(const float *P, const float *T, float *dP, float *loss, int64_t n, int32_t B,
+                       void *stream);
+/* One Adam step (step >= 1, bias-corrected) on FP32 master weights w; when
+ * w_bf16 is not NULL it receives the rounded weights. */
+PHI_API int phi_nn_adam(float *w, void *w_bf16, const float *g, float *m, float *v, int64_t n, float lr,
+                        float beta1, float beta2, float eps, int32_t step, void *stream);
+PHI_API int phi_nn_to_bf16(const float *a, void *b, int64_t n, void *stream);
+
+/* phi_gpu_steady_state from the initial hierarchy rho_0 = rho0_guess (host,
+ * 2*N*N doubles, column-major), every other node zero. */
+PHI_API int phi_gpu_steady_state_rho0(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode,
+                                      int32_t max_steps, const double *rho0_guess, phi_solve_stats *stats);
+
 #ifdef __cplusplus
 }
 #endif

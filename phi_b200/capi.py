@@ -134,6 +134,16 @@ SIGNATURES = [
     ("phi_gpu_batch_set_schedule", c_int, [c_void_p, POINTER(PhiBatchSchedule)]),
     ("phi_gpu_batch_rk4", c_int, [c_void_p, c_double, c_int64, POINTER(PhiBatchStats)]),
     ("phi_gpu_batch_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
+    ("phi_nn_linear_forward", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_int32,
+                                      c_int32, c_void_p]),
+    ("phi_nn_linear_backward", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                       c_int32, c_int32, c_int32, c_int32, c_void_p]),
+    ("phi_nn_mse", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int64, c_int32, c_void_p]),
+    ("phi_nn_adam", c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int64, ctypes.c_float,
+                            ctypes.c_float, ctypes.c_float, ctypes.c_float, c_int32, c_void_p]),
+    ("phi_nn_to_bf16", c_int, [c_void_p, c_void_p, c_int64, c_void_p]),
+    ("phi_gpu_steady_state_rho0", c_int, [c_void_p, c_int32, c_double, c_int32, c_int32, c_void_p,
+                                           POINTER(PhiSolveStats)]),
 ]
 
 _lib = None

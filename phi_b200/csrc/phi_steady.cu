@@ -69,10 +69,10 @@ const char *breakdown_text(int code) {
   }
 }
 
-}  // namespace
-
-extern "C" int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
-                                    const double *guess, phi_solve_stats *stats) {
+// guess: NULL (rho_0 = I/N), a whole hierarchy (guess_rho0 false) or rho_0
+// only (guess_rho0 true; other nodes zero).
+int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps, const double *guess,
+                bool guess_rho0, phi_solve_stats *stats) {
   if (!ctx) return PHI_E_INVALID;
   if (ell < 1 || ell > phi::kMaxEll) {
     ctx->error = "steady_state: ell must be in 1.." + std::to_string(phi::kMaxEll);
@@ -123,8 +123,11 @@ extern "C" int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32
   PHI_SK(phi::bicg_launch_rhs(V.b, n, grid, s));
   // x0: the caller's hierarchy, or rho_0 = I / N; scaled to x_0[0,0] = 1.
   std::vector<double2> rho;
-  if (guess) {
+  if (guess && !guess_rho0) {
     PHI_SK(cudaMemcpyAsync(V.x, guess, bytes, cudaMemcpyHostToDevice, s));
+  } else if (guess) {
+    PHI_SK(cudaMemsetAsync(V.x, 0, bytes, s));
+    PHI_SK(cudaMemcpyAsync(V.x, guess, (size_t)N * N * sizeof(double2), cudaMemcpyHostToDevice, s));
   } else {
     rho.assign((size_t)N * N, make_double2(0.0, 0.0));
     for (int i = 0; i < N; ++i) rho[(size_t)i * (N + 1)] = make_double2(1.0 / N, 0.0);
@@ -222,4 +225,20 @@ extern "C" int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32
     if (flag != PHI_OK) result = flag;
   }
   return result;
+}
+
+}  // namespace
+
+extern "C" int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
+                                    const double *guess, phi_solve_stats *stats) {
+  return steady_impl(ctx, ell, tol, tol_mode, max_steps, guess, false, stats);
+}
+
+extern "C" int phi_gpu_steady_state_rho0(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode,
+                                         int32_t max_steps, const double *rho0_guess, phi_solve_stats *stats) {
+  if (!rho0_guess) {
+    if (ctx) ctx->error = "steady_state_rho0: rho0_guess is NULL";
+    return PHI_E_INVALID;
+  }
+  return steady_impl(ctx, ell, tol, tol_mode, max_steps, rho0_guess, true, stats);
 }

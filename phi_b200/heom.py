@@ -292,18 +292,24 @@ class Hierarchy:
         self._check(self.lib.phi_gpu_reset(self.ctx, float(time)))
 
     def steady_state(self, tol: float = 1e-10, ell: int = 2, max_steps: int = 0, guess=None,
-                     tol_mode: int = capi.PHI_TOL_RELATIVE, check: bool = True):
+                     tol_mode: int = capi.PHI_TOL_RELATIVE, check: bool = True, rho0_guess=None):
         """BiCGSTAB(ell) steady state (L rho = 0, tr rho_0 = 1); the context
         state becomes the solution.  tol_mode: PHI_TOL_RELATIVE
         (||r|| <= tol ||b||), PHI_TOL_ABSOLUTE (||r|| <= tol) or
-        PHI_TOL_ABS_SQUARED (||r||^2 <= tol)."""
+        PHI_TOL_ABS_SQUARED (||r||^2 <= tol).  rho0_guess (N x N complex)
+        starts from that rho_0 with every other node zero."""
         st = capi.PhiSolveStats()
-        g = None
-        if guess is not None:
-            g = np.ascontiguousarray(guess, dtype=np.float64)
-            assert g.size == self.state_len
-        rc = self.lib.phi_gpu_steady_state(self.ctx, int(ell), float(tol), int(tol_mode), int(max_steps),
-                                           g.ctypes.data if g is not None else None, ctypes.byref(st))
+        if rho0_guess is not None:
+            g = col_major(rho0_guess)
+            rc = self.lib.phi_gpu_steady_state_rho0(self.ctx, int(ell), float(tol), int(tol_mode),
+                                                    int(max_steps), g.ctypes.data, ctypes.byref(st))
+        else:
+            g = None
+            if guess is not None:
+                g = np.ascontiguousarray(guess, dtype=np.float64)
+                assert g.size == self.state_len
+            rc = self.lib.phi_gpu_steady_state(self.ctx, int(ell), float(tol), int(tol_mode), int(max_steps),
+                                               g.ctypes.data if g is not None else None, ctypes.byref(st))
         if check:
             self._check(rc)
         return {"steps": st.iterations, "converged": bool(st.converged), "residual": st.residual,
