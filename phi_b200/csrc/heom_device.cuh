@@ -32,6 +32,7 @@ struct HeomConsts {
   int kind;         // BathKind
   int vacuum;       // truncation_level == 1: unitary part only
   int identity_sites;  // independent baths: bath m couples to |m><m|
+  int h_real;       // every Hamiltonian element has a zero imaginary part
   int64_t M;        // nodes
   double inv_hbar;  // 1 / hbar
   const uint8_t *mi;     // M*T

@@ -88,9 +88,9 @@ __global__ void __launch_bounds__(256, kBatchMinBlocks)
       if (threadIdx.x == 0 && err_flag) atomicOr(err_flag, 1);
       return;
     }
-    if (r == 0) {
+    if (r == 0) {  // both barriers completed one phase for this tile
       par0 ^= 1u;
-      if (p.npre > 0) par1 ^= 1u;
+      par1 ^= 1u;
     }
   }
 }

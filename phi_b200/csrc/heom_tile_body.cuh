@@ -181,7 +181,7 @@ struct TileMinBlocks {
 // has initialised the two mbarriers at the start of shared memory and passes
 // the phase parity each is at.  Returns 1 when the tile was skipped before
 // any copy was issued (RKF45 run finished), 0 when both barriers completed a
-// phase (barrier 1 only if p.npre > 0), -1 after a bounded wait gave up
+// phase (barrier 1 with 0 bytes when p.npre == 0), -1 after a bounded wait gave up
 // (err_flag set; the caller must stop).
 template <int N, int KT, bool MIXED>
 __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
@@ -192,16 +192,23 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES;
   const HeomConsts &c = p.c;
-  const int T = c.T;
+  constexpr int T = N * KT;  // PHI's identity site map: K+1 terms per site
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Lay::kBars);
   TX *Xs = reinterpret_cast<TX *>(smem_raw + Lay::kX);   // NT*ES
   TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*E
   unsigned char *PreBase = smem_raw + Lay::kPre;
-  size_t pre_off[kMaxPre];
+  // Byte offsets of the prefetched epilogue operands.  Every loop over them
+  // is unrolled so the offsets stay in registers.
+  uint32_t pre_off[kMaxPre];
   size_t tail = Lay::kPre;
-  for (int b = 0; b < kMaxPre; ++b) {
-    pre_off[b] = tail - Lay::kPre;
-    if (b < p.npre) tail += ((size_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
+  {
+    uint32_t acc_off = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      pre_off[b] = acc_off;
+      if (b < p.npre) acc_off += ((uint32_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
+    }
+    tail += acc_off;
   }
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
@@ -209,7 +216,8 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   R *cn = reinterpret_cast<R *>(coef + 24);                          // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
-  int *ids = reinterpret_cast<int *>(ccr + 2 * T);                  // NT*2T element offsets
+  R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element
+  int *ids = reinterpret_cast<int *>(mats + E);                     // NT*2T element offsets
   int *nts = ids + NT * 2 * T;                                      // NT*T
   unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
   unsigned char *pj = pi + P;
@@ -237,10 +245,15 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     mbar_expect_tx(&bars[0], xbytes);
     bulk_g2s(Xs, xin + n0 * ES, xbytes, &bars[0]);
     uint32_t pbytes = 0;
-    for (int b = 0; b < p.npre; ++b)
-      pbytes += (uint32_t)(nt_here * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b)
+      if (b < p.npre) pbytes += (uint32_t)(nt_here * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
+    // Arrives on barrier 1 in every tile (with 0 bytes when nothing is
+    // prefetched), so its phase advances once per tile like barrier 0's.
     mbar_expect_tx(&bars[1], pbytes);
-    for (int b = 0; b < p.npre; ++b) {
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      if (b >= p.npre) break;
       const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
       if (b == 0 && p.mode == kModeRkf45) src = reinterpret_cast<const unsigned char *>(p.ybuf[ycur]);
       const int stride = p.pre_bytes[b] == 16 ? E : ES;
@@ -248,7 +261,16 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       bulk_g2s(PreBase + pre_off[b], src + (size_t)n0 * stride * p.pre_bytes[b], bytes, &bars[1]);
     }
   }
-  for (int i = tid; i < E; i += 256) Hs[i] = from_d2<TX>(__ldg(c.H + i));
+  // A real Hamiltonian (every in-scope workload) is kept as E reals in the
+  // same buffer, halving the products of A = H X.
+  const bool hreal = c.h_real;
+  R *Hr = reinterpret_cast<R *>(Hs);
+  if (hreal) {
+    for (int i = tid; i < E; i += 256) Hr[i] = (R)__ldg(c.H + i).x;
+  } else {
+    for (int i = tid; i < E; i += 256) Hs[i] = from_d2<TX>(__ldg(c.H + i));
+  }
+  for (int i = tid; i < E; i += 256) mats[i] = (R)__ldg(c.mats_elem + i);
   for (int i = tid; i < P; i += 256) {
     pi[i] = __ldg(c.pair_i + i);
     pj[i] = __ldg(c.pair_j + i);
@@ -295,24 +317,36 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     const int i = pi[u], j = pj[u];
     const TX *X = Xs + nd * ES;
     R ar = 0, ai = 0, br = 0, bi = 0;  // A_ij, A_ji
+    if (hreal) {
 #pragma unroll
-    for (int k = 0; k < N; ++k) {
-      const TX hik = Hs[i + k * N], xkj = X[k + j * N];
-      const TX hjk = Hs[j + k * N], xki = X[k + i * N];
-      ar = fma(hik.x, xkj.x, ar);
-      ar = fma(-hik.y, xkj.y, ar);
-      ai = fma(hik.x, xkj.y, ai);
-      ai = fma(hik.y, xkj.x, ai);
-      br = fma(hjk.x, xki.x, br);
-      br = fma(-hjk.y, xki.y, br);
-      bi = fma(hjk.x, xki.y, bi);
-      bi = fma(hjk.y, xki.x, bi);
+      for (int k = 0; k < N; ++k) {
+        const R hik = Hr[i + k * N], hjk = Hr[j + k * N];
+        const TX xkj = X[k + j * N], xki = X[k + i * N];
+        ar = fma(hik, xkj.x, ar);
+        ai = fma(hik, xkj.y, ai);
+        br = fma(hjk, xki.x, br);
+        bi = fma(hjk, xki.y, bi);
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < N; ++k) {
+        const TX hik = Hs[i + k * N], xkj = X[k + j * N];
+        const TX hjk = Hs[j + k * N], xki = X[k + i * N];
+        ar = fma(hik.x, xkj.x, ar);
+        ar = fma(-hik.y, xkj.y, ar);
+        ai = fma(hik.x, xkj.y, ai);
+        ai = fma(hik.y, xkj.x, ai);
+        br = fma(hjk.x, xki.x, br);
+        br = fma(-hjk.y, xki.y, br);
+        bi = fma(hjk.x, xki.y, bi);
+        bi = fma(hjk.y, xki.x, bi);
+      }
     }
     // -i/hbar (A_ij - conj(A_ji))
     R vx = (ai + bi) * ih, vy = -(ar - br) * ih;
     const TX xij = X[i + j * N];
     if (!c.vacuum) {
-      const R fac = (R)(deph[nd] + __ldg(c.mats_elem + i + j * N));
+      const R fac = (R)deph[nd] + mats[i + j * N];
       vx = fma(-fac, xij.x, vx);
       vy = fma(-fac, xij.y, vy);
       const int *nid = ids + nd * 2 * T;
@@ -444,7 +478,9 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         st_stream(static_cast<TX *>(p.k[s]) + gx, kx);
         const int row = s * (s + 1) / 2;
         double2 xv = ys;
-        for (int r = 0; r < s; ++r) xv = cfma(xv, to_d2(preX(1 + r)[nd * ES + w]), cf[row + r]);
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (r < s) xv = cfma(xv, to_d2(preX(1 + r)[nd * ES + w]), cf[row + r]);
         xv = cfma(xv, kv, cf[row + s]);
         out[gx] = from_d2<TX>(xv);
       } else {      // pre = {y, k0, k2, k3, k4}
@@ -487,7 +523,7 @@ inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
   b += (size_t)(S::NT + 24) * sizeof(double);
-  b += (size_t)(2 * S::NT * T + 2 * T) * Lay::XB / 2;  // cn, cp, ccr in the arithmetic type
+  b += (size_t)(2 * S::NT * T + 2 * T + S::E) * Lay::XB / 2;  // cn, cp, ccr, mats in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;
   return b;

@@ -205,6 +205,9 @@ int setup_constants(phi_ctx *ctx) {
     for (int b = 0; b < nb; ++b)
       if (ctx->bath_sites[b] != b) c.identity_sites = 0;
   }
+  c.h_real = 1;
+  for (int k = 0; k < N * N; ++k)
+    if (ctx->hamiltonian[2 * k + 1] != 0.0) c.h_real = 0;
   c.M = ctx->hier.M;
   c.inv_hbar = 1.0 / hbar;
   c.mi = ctx->hier.mi.as<uint8_t>();
