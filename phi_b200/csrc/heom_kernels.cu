@@ -405,7 +405,15 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
       const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
       bits = o > bits ? o : bits;
     }
-    if ((threadIdx.x & 31) == 0 && bits) atomicMax(&p.ctl->err_bits, bits);
+    // one atomic per CTA (every CTA updates the same error word)
+    __shared__ unsigned long long wmax[8];
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = bits;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned long long m = wmax[0];
+      for (int w = 1; w < 8; ++w) m = wmax[w] > m ? wmax[w] : m;
+      if (m) atomicMax(&p.ctl->err_bits, m);
+    }
   }
 }
 

@@ -213,7 +213,8 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
   double *coef = deph + NT;                                         // 24
-  R *cn = reinterpret_cast<R *>(coef + 24);                          // NT*T |next prefactor|
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // 8 warp maxima
+  R *cn = reinterpret_cast<R *>(wmax + 8);                           // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
   R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element
@@ -508,7 +509,16 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
         bits = o > bits ? o : bits;
       }
-      if ((tid & 31) == 0 && bits) atomicMax(&p.ctl->err_bits, bits);
+      // One atomic per CTA: a single error word takes every CTA's maximum,
+      // so per-warp atomics would serialise tens of thousands of updates.
+      if ((tid & 31) == 0) wmax[tid >> 5] = bits;
+      __syncthreads();
+      if (tid == 0) {
+        unsigned long long m = wmax[0];
+#pragma unroll
+        for (int w = 1; w < 8; ++w) m = wmax[w] > m ? wmax[w] : m;
+        if (m) atomicMax(&p.ctl->err_bits, m);
+      }
     }
   }
   return 0;
@@ -522,7 +532,7 @@ inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
   for (int i = 0; i < npre; ++i)
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
-  b += (size_t)(S::NT + 24) * sizeof(double);
+  b += (size_t)(S::NT + 24 + 8) * sizeof(double);  // deph, coef, warp maxima
   b += (size_t)(2 * S::NT * T + 2 * T + S::E) * Lay::XB / 2;  // cn, cp, ccr, mats in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;
