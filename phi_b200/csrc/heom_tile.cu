@@ -15,7 +15,7 @@ using namespace tile_detail;
 namespace {
 
 template <int N, int KT, bool MIXED>
-__global__ void __launch_bounds__(256, TileMinBlocks<KT>::value) heom_tile_kernel(TileParams p) {
+__global__ void __launch_bounds__(256, TileMinBlocks<KT, MIXED>::value) heom_tile_kernel(TileParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   tile_init_barriers(smem_raw);
   tile_body<N, KT, MIXED>(p, blockIdx.x, smem_raw, 0u, 0u);
