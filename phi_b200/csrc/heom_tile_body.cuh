@@ -153,6 +153,10 @@ struct TileShape {
   static constexpr int P = N * (N + 1) / 2;
   static constexpr int NT0 = 256 / P;     // about one (node, pair) item per thread
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
+  // Column stride of the derivative tile in shared memory: odd, so the
+  // transposed (j, i) writes of one warp fall in distinct banks.
+  static constexpr int NP = (N & 1) ? N : N + 1;
+  static constexpr int EU = N * NP;
 };
 
 template <int N, bool MIXED>
@@ -165,7 +169,7 @@ struct TileLayout {
   static constexpr size_t kX = 128;
   static constexpr size_t kXBytes = ((size_t)S::NT * ES * XB + 127) / 128 * 128;
   static constexpr size_t kU = kX + kXBytes;
-  static constexpr size_t kUBytes = ((size_t)S::NT * S::E * XB + 127) / 128 * 128;
+  static constexpr size_t kUBytes = ((size_t)S::NT * S::EU * XB + 127) / 128 * 128;
   static constexpr size_t kPre = kU + kUBytes;
 };
 
@@ -192,12 +196,19 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   using Lay = TileLayout<N, MIXED>;
   using TX = typename std::conditional<MIXED, float2, double2>::type;
   using R = typename std::conditional<MIXED, float, double>::type;
-  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES;
+  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES, NP = S::NP, EU = S::EU;
+  // tile element e (node e / E, column-major offset e % E) in the padded
+  // derivative tile
+  auto uix = [](int e) {
+    if (NP == N) return e;
+    const int nd = e / E, w = e - nd * E, c = w / N;
+    return nd * EU + (w - c * N) + c * NP;
+  };
   const HeomConsts &c = p.c;
   constexpr int T = N * KT;  // PHI's identity site map: K+1 terms per site
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Lay::kBars);
   TX *Xs = reinterpret_cast<TX *>(smem_raw + Lay::kX);   // NT*ES
-  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*E
+  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*EU (column stride NP)
   unsigned char *PreBase = smem_raw + Lay::kPre;
   // Byte offsets of the prefetched epilogue operands.  Every loop over them
   // is unrolled so the offsets stay in registers.
@@ -323,26 +334,28 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     if (hreal) {
 #pragma unroll
       for (int k = 0; k < N; ++k) {
+        // X_ki = conj(X_ik) (Hermitian ADO): lanes with consecutive i read
+        // consecutive words instead of a stride of N.
         const R hik = Hr[i + k * N], hjk = Hr[j + k * N];
-        const TX xkj = X[k + j * N], xki = X[k + i * N];
+        const TX xkj = X[k + j * N], xik = X[i + k * N];
         ar = fma(hik, xkj.x, ar);
         ai = fma(hik, xkj.y, ai);
-        br = fma(hjk, xki.x, br);
-        bi = fma(hjk, xki.y, bi);
+        br = fma(hjk, xik.x, br);
+        bi = fma(-hjk, xik.y, bi);
       }
     } else {
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         const TX hik = Hs[i + k * N], xkj = X[k + j * N];
-        const TX hjk = Hs[j + k * N], xki = X[k + i * N];
+        const TX hjk = Hs[j + k * N], xik = X[i + k * N];  // X_ki = conj(X_ik)
         ar = fma(hik.x, xkj.x, ar);
         ar = fma(-hik.y, xkj.y, ar);
         ai = fma(hik.x, xkj.y, ai);
         ai = fma(hik.y, xkj.x, ai);
-        br = fma(hjk.x, xki.x, br);
-        br = fma(-hjk.y, xki.y, br);
-        bi = fma(hjk.x, xki.y, bi);
-        bi = fma(hjk.y, xki.x, bi);
+        br = fma(hjk.x, xik.x, br);
+        br = fma(hjk.y, xik.y, br);
+        bi = fma(-hjk.x, xik.y, bi);
+        bi = fma(hjk.y, xik.x, bi);
       }
     }
     // -i/hbar (A_ij - conj(A_ji))
@@ -408,11 +421,11 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     v.y = vy;
     if (i == j) {
       v.y = 0;
-      Us[nd * E + i + j * N] = v;
+      Us[nd * EU + i + j * NP] = v;
     } else {
-      Us[nd * E + i + j * N] = v;
+      Us[nd * EU + i + j * NP] = v;
       v.y = -v.y;
-      Us[nd * E + j + i * N] = v;
+      Us[nd * EU + j + i * NP] = v;
     }
   }
   ok = p.npre == 0 || mbar_wait_bounded(&bars[1], par1);
@@ -431,7 +444,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     TX *out = static_cast<TX *>(p.out);
     for (int e = tid; e < tile_elems; e += 256) {
       const int nd = e / E, w = e - nd * E;
-      st_stream(out + (n0 + nd) * ES + w, Us[e]);
+      st_stream(out + (n0 + nd) * ES + w, Us[uix(e)]);
     }
   } else if (p.mode == kModeRk4) {
     const int s = p.stage;
@@ -444,7 +457,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     for (int e = tid; e < tile_elems; e += 256) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
-      const double2 kv = to_d2(Us[e]);
+      const double2 kv = to_d2(Us[uix(e)]);
       if (s == 0) {  // FP64: pre = {} (y is the input); MIXED: pre = {y}
         const double2 ys = MIXED ? preD(0)[e] : to_d2(Xs[nd * ES + w]);
         out[gx] = from_d2<TX>(cfma(ys, kv, p.a_next));
@@ -474,7 +487,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     for (int e = tid; e < tile_elems; e += 256) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
-      const TX kx = Us[e];
+      const TX kx = Us[uix(e)];
       const double2 kv = to_d2(kx);
       if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; FP64 stage 0: y is the input
         const double2 ys = (s == 0 && !MIXED) ? to_d2(Xs[nd * ES + w]) : preD(0)[e];
