@@ -50,15 +50,28 @@ def parse_args():
     ap.add_argument("--impl", default="phi_b200", choices=["phi_b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="frenkel7", choices=["frenkel7", "batched"],
-                    help="frenkel7: the RKF45 headline; batched: 512 uneven RK4 instances")
+    ap.add_argument("--workload", default="frenkel7", choices=["frenkel7", "ring24", "batched", "steady"],
+                    help="frenkel7: the RKF45 headline (7-site exciton); ring24: 24-site ring RKF45; "
+                         "batched: 512 uneven RK4 instances; steady: chain4 steady states, plain vs "
+                         "learned initial guess")
     ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--draws", type=int, default=32, help="steady workload: held-out draws")
     return ap.parse_args()
+
+
+# RKF45 workloads: maker, t_end (ps), description.
+RKF45_WORKLOADS = {
+    "frenkel7": ("frenkel7", 1.0, "frenkel7_K1_L6: 7-site Frenkel exciton, 7 Drude baths, K=1, L=6, "
+                                  "38760 nodes of 7x7, RKF45 tol 1e-6 to 1 ps"),
+    "ring24": ("ring24", 0.5, "ring24_K0_L4: 24-site ring, 24 Drude baths, K=0, L=4, 20475 nodes of "
+                              "24x24, RKF45 tol 1e-6 to 500 fs"),
+}
+WORKLOAD = "frenkel7"
 
 
 def workload():
     from phi_b200 import configs
-    p = configs.frenkel7()
+    p = getattr(configs, RKF45_WORKLOADS[WORKLOAD][0])()
     p.fix_incompatible_combinations("rkf45")
     return p
 
@@ -166,8 +179,7 @@ def run_reference_arm(args):
     res = {"impl": "reference", "metric": METRIC, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-           "config": {"workload": "frenkel7_K1_L6 (N=7, 7 Drude baths, 38760 nodes), RKF45 tol 1e-6",
-                      "seed": p.seed, "threads": threads}}
+           "config": {"workload": RKF45_WORKLOADS[WORKLOAD][2], "seed": p.seed, "threads": threads}}
     if not O.ref_available():
         res["unavailable"] = "reference build oracle/_ref/ref_driver not present"
         return res
@@ -197,7 +209,9 @@ def run_reference_arm(args):
     if sa is None or sb is None or sb <= sa or wb <= wa:
         res["unavailable"] = f"could not difference the reference runs: {runs}"
         return res
-    M = 38760
+    from phi_b200 import configs
+    M = configs.hierarchy_nodes(int(p.num_bath_couplings) * int(p.num_matsubara_terms),
+                                int(p.hierarchy_truncation_level) - 1)
     per_step = (wb - wa) / (sb - sa)
     value = 6 * M / per_step
     res.update({"value": value, "ms_per_step": per_step * 1e3,
@@ -344,13 +358,54 @@ def run_batched(args):
         dist.destroy_process_group()
 
 
+def run_steady(args):
+    """chain4 steady states (4-site chain, K=2, depth 8: 125,970 nodes of
+    4x4): BiCGSTAB(2) to ||r||/||b|| <= 1e-10 from I/N, from the thermal
+    state and from the learned rho_0, on `--draws` held-out draws; value =
+    node-applies/s of the plain solves (2 applies per BiCG step)."""
+    import numpy as np
+    import torch
+    from phi_b200 import train_guess
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    res = train_guess.evaluate(args.draws)
+    rows = [r for r in res["rows"] if r["plain_ok"] and r["learned_ok"]]
+    M = 125970
+    plain_s = sum(r["plain_device_s"] for r in rows)
+    plain_steps = sum(r["plain_steps"] for r in rows)
+    value = 2 * M * plain_steps / plain_s if plain_s else None
+    out = {"metric": "steady-state solve: node-applies/s and wall time to ||r||/||b|| <= 1e-10",
+           "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.draws, "warmup": 0,
+           "ms_per_step": 1e3 * plain_s / max(len(rows), 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "c128", "data": "synthetic (chain4 family, seeds 1000+)",
+           "config": {"workload": "chain4_K2_L8: 4-site chain, 4 Drude baths, K=2, L=8, 125970 nodes of 4x4; "
+                                  "BiCGSTAB(2), relative residual 1e-10", "draws": args.draws},
+           "learned_vs_plain": {k: v for k, v in res.items() if k != "rows"},
+           "gpu_launches": None}
+    print(json.dumps(out), flush=True)
+
+
 def main():
+    global WORKLOAD, T_END
     args = parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.workload == "batched" and args.impl != "reference":
+    if args.impl == "reference" and args.workload in ("batched", "steady"):
+        if int(os.environ.get("RANK", "0")) == 0:
+            why = ("the reference's steady-state solvers crash or return NaN on in-scope inputs"
+                   if args.workload == "steady" else
+                   "not timed for this workload: the reference integrates one problem per process "
+                   "(its CPU path is timed on the frenkel7 and ring24 workloads)")
+            print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    if args.workload == "batched":
         run_batched(args)
         return
+    if args.workload == "steady":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_steady(args)
+        return
+    WORKLOAD = args.workload
+    T_END = RKF45_WORKLOADS[WORKLOAD][1]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -378,6 +433,7 @@ def main():
     # ---- device-resident throughput (value) ----
     h = Hierarchy(p, precision=prec, device=local_rank)
     M = h.num_nodes
+    T_terms = h.num_terms
     stream = torch.cuda.ExternalStream(h.stream_handle(), device=local_rank)
     run_steps(h, args.warmup, True)
     torch.cuda.synchronize()
@@ -451,7 +507,7 @@ def main():
         t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_value = 6 * M * e2e_steps * world / float(t.item())
-    h2d = (2 * E + 2 * E + 2 * 7) * 8  # H, rho(0), gamma, lambda
+    h2d = (2 * E + 2 * E + 2 * int(p.num_bath_couplings)) * 8  # H, rho(0), gamma, lambda
     d2h = 2 * E * 8 + ((e2e_steps + 15) // 16 + 1) * 320  # rho_0 + control-block polls
 
     # ---- the other arithmetic, and the full 1 ps rho_0 error of mixed vs FP64 ----
@@ -488,7 +544,7 @@ def main():
         apply_gbs = apply_bytes / (apply_ms / 1e3) / 1e9
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath):
+        if os.path.exists(tpath) and WORKLOAD == "frenkel7":
             try:
                 traffic = json.load(open(tpath)).get("rkf45_step_dram_bytes")
             except Exception:
@@ -498,12 +554,12 @@ def main():
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "c128" if prec == capi.PHI_PREC_FP64 else "c64 stages (fp32 Liouvillian) + c128 state/norms",
-            "data": "synthetic (seeded frenkel7, numpy default_rng seed 7)",
-            "config": {"workload": "frenkel7_K1_L6: 7-site Frenkel exciton, 7 Drude baths, K=1, L=6, "
-                                   "38760 nodes of 7x7, RKF45 tol 1e-6 to 1 ps",
-                       "nodes": M, "num_states": N, "terms": h.num_terms if False else 14,
+            "data": f"synthetic (seeded {WORKLOAD}, numpy default_rng seed {p.seed})",
+            "config": {"workload": RKF45_WORKLOADS[WORKLOAD][2],
+                       "nodes": M, "num_states": N, "terms": T_terms,
                        "precision": args.precision, "parallelism": f"replicas x{world}",
-                       "l2": "working set 9 x 30.4 MB state buffers = 274 MB > 126 MB L2"},
+                       "l2": f"working set 9 x {M * E * 16 / 1e6:.1f} MB state buffers = "
+                             f"{9 * M * E * 16 / 1e6:.0f} MB > 126 MB L2"},
             "rkf45_steps_per_s": total_steps / (t_max / 1e3),
             "rho0_err_vs_fp64": rho_err,
             "meets_1e-6": rho_err <= 1e-6,
