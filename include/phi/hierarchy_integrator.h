@@ -61,6 +61,7 @@ class PHI_API HierarchyIntegrator {
   void RunRk4(std::ofstream &out);
   void RunRkf45(std::ofstream &out);
   void RunSteadyState(std::ofstream &out);
+  void WriteRestartIfAsked(double timestep);
   void Fail(int code, const std::string &msg);
 };
 

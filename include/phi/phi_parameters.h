@@ -76,6 +76,7 @@ struct PHI_API PhiParameters {
   Float rkf45_tolerance;
   Float bicgstab_tolerance;
   Float filter_tolerance;
+  Float restart_output_time;  // RestartOutputTimeSecs: > 0 writes RestartFile at the end of a run
 
   std::string output_filename;
   std::string restart_input_filename;

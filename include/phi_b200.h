@@ -235,6 +235,27 @@ PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out
  * create when ctx is NULL) into buf. */
 PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
 
+/* ---- Restart files --------------------------------------------------------
+ * PHI's restart layout (RestartHelper::WriteRestartFile / ReadRestartFile,
+ * restart_helper.cc:30-84): the time, the step size, then one line per node
+ * with its N*N elements in storage order as "(re,im)".  Written with 17
+ * significant digits (PHI writes 6); read in either form.  Files that also
+ * hold time-local truncation matrices are rejected.  The host functions work
+ * on host buffers of 2*M*N*N doubles and need no GPU. */
+PHI_API int phi_restart_read_file(const char *path, int32_t num_states, int64_t num_nodes, double *state,
+                                  double *time, double *timestep);
+PHI_API int phi_restart_write_file(const char *path, int32_t num_states, int64_t num_nodes, const double *state,
+                                   double time, double timestep);
+PHI_API int phi_restart_last_error(char *buf, size_t len);
+/* The context's state and time to / from a restart file (RestartInput and
+ * RestartFile of PHI's parameter file). */
+PHI_API int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double timestep);
+PHI_API int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *timestep);
+/* Binary fast path: "PHIB200S", uint32 version 1, uint32 N, int64 M, double
+ * time, double step size, then the 2*M*N*N doubles of the state. */
+PHI_API int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timestep);
+PHI_API int phi_gpu_load_state(phi_ctx *ctx, const char *path, double *timestep);
+
 /* ---- Batched instances ------------------------------------------------
  * Many independent hierarchies of uneven N, K and depth integrated together
  * (the reference runs one problem per process; this replaces a loop of

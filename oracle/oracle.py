@@ -325,12 +325,18 @@ def run_reference(p, method: str, threads: int = 1, timeout: float = 600.0, **kw
             f.write(param_file_text(p, **kw))
         subprocess.run([REF_DRIVER, "run", prm, method, str(threads), out], check=True,
                        timeout=timeout, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
-        with open(out) as f:
-            lines = f.read().split("\n")
-    secs = float(lines[0].split()[1])
+        secs = float(open(out).read().split("\n")[0].split()[1])
+        return parse_rho_file(out, n), secs
+
+
+def parse_rho_file(path: str, n: int) -> np.ndarray:
+    """rho_0 as ref_driver prints it (a timing line, a header, then N*N
+    `re im` lines in column-major order)."""
+    with open(path) as f:
+        lines = f.read().split("\n")
     vals = np.array([[float(x) for x in ln.split()] for ln in lines[2:2 + n * n]])
     rho_cm = vals[:, 0] + 1j * vals[:, 1]
-    return rho_cm.reshape(n, n).T.copy(), secs
+    return rho_cm.reshape(n, n).T.copy()
 
 
 def reference_order(p, timeout: float = 600.0) -> np.ndarray:

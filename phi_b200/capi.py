@@ -127,6 +127,13 @@ SIGNATURES = [
     ("phi_gpu_reset", c_int, [c_void_p, c_double]),
     ("phi_gpu_rk4_step_noalloc", c_int, [c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
+    ("phi_restart_read_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, POINTER(c_double), POINTER(c_double)]),
+    ("phi_restart_write_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, c_double, c_double]),
+    ("phi_restart_last_error", c_int, [c_char_p, c_size_t]),
+    ("phi_gpu_write_restart", c_int, [c_void_p, c_char_p, c_double]),
+    ("phi_gpu_read_restart", c_int, [c_void_p, c_char_p, POINTER(c_double)]),
+    ("phi_gpu_save_state", c_int, [c_void_p, c_char_p, c_double]),
+    ("phi_gpu_load_state", c_int, [c_void_p, c_char_p, POINTER(c_double)]),
     ("phi_gpu_batch_create", c_int, [POINTER(PhiProblemDesc), c_int32, POINTER(c_void_p)]),
     ("phi_gpu_batch_destroy", c_int, [c_void_p]),
     ("phi_gpu_batch_instance", c_int, [c_void_p, c_int32, POINTER(c_void_p)]),
@@ -185,6 +192,37 @@ def last_error(ctx=None) -> str:
 def check(code: int, ctx=None) -> None:
     if code != PHI_OK:
         raise PhiError(code, last_error(ctx))
+
+
+def restart_last_error() -> str:
+    lib = load()
+    buf = ctypes.create_string_buffer(1024)
+    lib.phi_restart_last_error(buf, 1024)
+    return buf.value.decode(errors="replace")
+
+
+def restart_read(path: str, num_states: int, num_nodes: int):
+    """PHI restart file -> (state as 2*M*N*N doubles, time, step size)."""
+    import numpy as np
+    lib = load()
+    st = np.zeros(2 * num_nodes * num_states * num_states)
+    t, dt = c_double(), c_double()
+    rc = lib.phi_restart_read_file(str(path).encode(), num_states, num_nodes, st.ctypes.data, ctypes.byref(t),
+                                   ctypes.byref(dt))
+    if rc != PHI_OK:
+        raise PhiError(rc, restart_last_error())
+    return st, t.value, dt.value
+
+
+def restart_write(path: str, num_states: int, num_nodes: int, state, time: float, timestep: float):
+    import numpy as np
+    lib = load()
+    st = np.ascontiguousarray(state, dtype=np.float64)
+    assert st.size == 2 * num_nodes * num_states * num_states
+    rc = lib.phi_restart_write_file(str(path).encode(), num_states, num_nodes, st.ctypes.data, float(time),
+                                    float(timestep))
+    if rc != PHI_OK:
+        raise PhiError(rc, restart_last_error())
 
 
 def batch_last_error(batch=None) -> str:

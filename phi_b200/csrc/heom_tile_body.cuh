@@ -151,7 +151,9 @@ struct TileShape {
   static constexpr int E = N * N;
   static constexpr int EP = E + (E & 1);  // complex64 node stride (16-byte aligned nodes)
   static constexpr int P = N * (N + 1) / 2;
-  static constexpr int NT0 = 256 / P;     // about one (node, pair) item per thread
+  // About one (node, pair) item per thread; two for N >= 12, whose nodes
+  // would otherwise leave a tile of one node and idle threads.
+  static constexpr int NT0 = (N >= 12 ? 512 : 256) / P;
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
   // Column stride of the derivative tile in shared memory: odd, so the
   // transposed (j, i) writes of one warp fall in distinct banks.

@@ -28,10 +28,9 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
     return reject("Hilbert-space truncation is outside this library's scope");
   if (p.use_time_local_truncation) return reject("time-local truncation is outside this library's scope");
   if (p.filter_tolerance > 0) return reject("adaptive hierarchy filtering is outside this library's scope");
-  if (p.is_restarted) return reject("restart input is outside this library's scope");
   if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
   const bool steady = p.run_method == BICGSTAB || p.run_method == BICGSTABL || p.run_method == BICGSTABU;
-  if (p.initial_density_matrix == nullptr && !steady)
+  if (p.initial_density_matrix == nullptr && !steady && !p.is_restarted)
     return reject("InitialDensityMatrix is required (the thermal guess needs LAPACK and is not supported)");
   if (p.gamma == nullptr || p.lambda == nullptr) return reject("Gamma and Lambda are required");
   *d = phi_problem_desc{};
@@ -119,6 +118,23 @@ void HierarchyIntegrator::Run(int, int, RunMethod method) {
   }
   if (!Prepare()) return;
   const int N = parameters_->num_states;
+  if (parameters_->is_restarted && !steady) {
+    // InitializeDensityMatrix with RestartInput (hierarchy_integrator.cc:
+    // 1045-1061): the whole hierarchy, the start time and the step size
+    // come from the restart file.
+    double dt = parameters_->timestep;
+    int rc = phi_gpu_read_restart(ctx_, parameters_->restart_input_filename.c_str(), &dt);
+    if (rc != PHI_OK) {
+      char buf[512];
+      phi_restart_last_error(buf, sizeof buf);
+      Fail(rc, std::string("RestartInput: ") + buf);
+      return;
+    }
+    double t0 = parameters_->start_time;
+    phi_gpu_get_time(ctx_, &t0);
+    parameters_->start_time = t0;
+    parameters_->timestep = dt;
+  }
   int64_t M = 0;
   phi_gpu_dims(ctx_, &M, nullptr, nullptr);
   std::ofstream out;
@@ -133,7 +149,9 @@ void HierarchyIntegrator::Run(int, int, RunMethod method) {
     out << "#-------------\n";
     if (!steady) {
       out << parameters_->start_time << " ";
-      for (int i = 0; i < N * N; ++i) out << parameters_->initial_density_matrix[i] << " ";
+      std::vector<Complex> rho0((size_t)N * N);
+      phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(rho0.data()));  // rho(0) or the restart's rho_0
+      for (int i = 0; i < N * N; ++i) out << rho0[i] << " ";
       out << "\n";
     }
     out << std::flush;
@@ -181,6 +199,7 @@ void HierarchyIntegrator::RunRk4(std::ofstream &out) {
   }
   steps_ = nsteps;
   accepted_ = nsteps;
+  WriteRestartIfAsked(dt);
   if (!out.is_open()) return;
   const Complex *rows_c = reinterpret_cast<const Complex *>(traj.data());
   for (long long r = 0; r < std::min<long long>(nout, rows); ++r) {
@@ -217,6 +236,7 @@ void HierarchyIntegrator::RunRkf45(std::ofstream &out) {
   }
   steps_ = st.steps;
   accepted_ = st.accepted;
+  WriteRestartIfAsked(st.final_dt);
   if (!out.is_open()) return;
   std::vector<Complex> rho((size_t)N * N);
   phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(rho.data()));
@@ -280,6 +300,21 @@ void HierarchyIntegrator::RunSteadyState(std::ofstream &out) {
   out << st.iterations << " ";
   for (int j = 0; j < N * N; ++j) out << rho[j] << " ";
   out << std::endl;
+}
+
+// The closing restart file of Rk4Integrate / Rkf45Integrate
+// (hierarchy_integrator.cc:2559-2563, :2925-2929): written when
+// RestartOutputTimeSecs > 0.  The periodic wall-clock writes during a run are
+// not made: a run is one device call.
+void HierarchyIntegrator::WriteRestartIfAsked(double timestep) {
+  const PhiParameters &p = *parameters_;
+  if (!(p.restart_output_time > 0) || p.restart_output_filename.empty()) return;
+  const int rc = phi_gpu_write_restart(ctx_, p.restart_output_filename.c_str(), timestep);
+  if (rc != PHI_OK) {
+    char buf[512];
+    phi_restart_last_error(buf, sizeof buf);
+    Fail(rc, std::string("RestartFile: ") + buf);
+  }
 }
 
 Complex *HierarchyIntegrator::density_matrix() {

@@ -208,6 +208,7 @@ void PhiParameters::SetDefaults() {
   is_full_bath_coupling = false;
   is_rho_normalized = true;
   is_restarted = false;
+  restart_output_time = 0;
   has_kappa = false;
   bicgstab_ell = 2;
   num_threads = 1;
@@ -400,6 +401,8 @@ void PhiParameters::ReadInputFile(std::string parameter_file) {
       verbose = std::atoi(trim(val).c_str());
     } else if (key == "RestartFile") {
       restart_output_filename = trim(val);
+    } else if (key == "RestartOutputTimeSecs") {
+      if (!parse_double(val, key, &restart_output_time, kNonNegative)) { are_parameters_valid = false; break; }
     } else if (key == "tol_low" || key == "RKF45mindt") {
       if (!parse_double(val, key, &rkf45_minimum_timestep, kPositive)) { are_parameters_valid = false; break; }
       if (key == "tol_low") bicgstab_tolerance = rkf45_minimum_timestep;

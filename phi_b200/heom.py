@@ -282,6 +282,29 @@ class Hierarchy:
         return {"steps": st.steps, "accepted": st.accepted, "final_time": st.final_time,
                 "final_dt": st.final_dt, "max_error": st.max_error}
 
+    def _restart_check(self, rc):
+        if rc != capi.PHI_OK:
+            raise capi.PhiError(rc, capi.restart_last_error() or capi.last_error(self.ctx))
+
+    def write_restart(self, path: str, timestep: float) -> None:
+        """PHI restart file of the state and time (17 significant digits)."""
+        self._restart_check(self.lib.phi_gpu_write_restart(self.ctx, str(path).encode(), float(timestep)))
+
+    def read_restart(self, path: str) -> float:
+        """State and time from a PHI restart file; returns its step size."""
+        dt = ctypes.c_double()
+        self._restart_check(self.lib.phi_gpu_read_restart(self.ctx, str(path).encode(), ctypes.byref(dt)))
+        return dt.value
+
+    def save_state(self, path: str, timestep: float = 0.0) -> None:
+        """Binary state file (exact)."""
+        self._restart_check(self.lib.phi_gpu_save_state(self.ctx, str(path).encode(), float(timestep)))
+
+    def load_state(self, path: str) -> float:
+        dt = ctypes.c_double()
+        self._restart_check(self.lib.phi_gpu_load_state(self.ctx, str(path).encode(), ctypes.byref(dt)))
+        return dt.value
+
     def stream_handle(self) -> int:
         s = ctypes.c_void_p()
         self._check(self.lib.phi_gpu_stream(self.ctx, ctypes.byref(s)))

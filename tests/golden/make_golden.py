@@ -12,12 +12,20 @@ Outputs (committed; the GPU host has no reference tree):
                         the problems listed in CASES (builder + arguments)
   ref_order.json        node order of the reference's ConstructI for a set of
                         (terms, truncation) pairs
+  ref_restart_indep_n3.txt / .json
+                        a restart file written by the reference build
+                        (RestartFile, RestartOutputTimeSecs; restart_helper.cc
+                        :30-53) at the end of an RK4 run, with the run's
+                        parameters and its rho_0 printed with %.17g
+
+    python tests/golden/make_golden.py /root/reference restart   # restart fixture only
 """
 from __future__ import annotations
 
 import json
 import os
 import re
+import tempfile
 import subprocess
 import sys
 
@@ -83,10 +91,38 @@ def parse_reference_tests(ref_root: str) -> dict:
     return out
 
 
+RESTART_CASE = ("random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=3), 0.001, 0.01)
+
+
+def make_restart_fixture():
+    builder, kw, dt, t_end = RESTART_CASE
+    p = build(builder, kw)
+    with tempfile.TemporaryDirectory() as d:
+        prm, out, rst, rho_f = (os.path.join(d, x) for x in ("in.prm", "out.txt", "restart.txt", "rho.txt"))
+        with open(prm, "w") as f:
+            f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_file=out)
+                    + f"RestartFile={rst}\nRestartOutputTimeSecs=1\n")
+        subprocess.run([O.REF_DRIVER, "run", prm, "rk4", "1", rho_f], check=True, timeout=120,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        text = open(rst).read()
+        rho = O.parse_rho_file(rho_f, p.num_states)
+    with open(os.path.join(HERE, "ref_restart_indep_n3.txt"), "w") as f:
+        f.write(text)
+    with open(os.path.join(HERE, "ref_restart_indep_n3.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "builder": builder, "kwargs": kw,
+                   "method": "rk4", "timestep": dt, "t_end": t_end,
+                   "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}, f, indent=0)
+    print("restart fixture written", flush=True)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
         raise SystemExit("build the reference first: make -C oracle")
+    if len(sys.argv) > 2 and sys.argv[2] == "restart":
+        make_restart_fixture()
+        return
+    make_restart_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)
