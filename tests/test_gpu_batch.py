@@ -100,3 +100,23 @@ def test_batch_rejects_instances_without_tile_kernel():
     probs.append(configs.spin_boson())  # DiagonalBath
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
         Batch(probs)
+
+
+def test_batch_covers_every_tile_instantiation():
+    """Instances of every tile-kernel N with K+1 = 1, 2 and 3 in one launch,
+    each equal to its own context bit for bit."""
+    import cases
+    probs = []
+    seed = 100
+    for n in (2, 3, 4, 5, 6, 7, 8, 10, 12, 16, 24):
+        for k1 in (1, 2, 3):
+            depth = 2 if n >= 10 or k1 == 3 else 3
+            probs.append(cases.random_problem("independent", n=n, matsubara=k1, truncation=depth + 1,
+                                              seed=seed))
+            seed += 1
+    with Batch(probs) as b:
+        b.rk4(DT, 5)
+        got = [b[i].get_state() for i in range(b.count)]
+    for i, p in enumerate(probs):
+        ref, _ = _alone(p, 5)
+        assert np.array_equal(got[i], ref), (i, p.num_states, p.num_matsubara_terms)
