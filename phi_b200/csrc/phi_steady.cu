@@ -59,6 +59,15 @@ cudaError_t outer_iteration(phi_ctx *ctx, const phi::BicgVectors &V, long long n
   return e;
 }
 
+// Owns the timing events of one solve.
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+
 const char *breakdown_text(int code) {
   switch (code) {
     case phi::kBicgRhoZero: return "BiCGSTAB breakdown: <rhat, r> = 0";
@@ -111,9 +120,10 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
   cudaStream_t s = ctx->stream;
   const int grid = phi::bicg_grid(ctx->num_sms);
 
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-  PHI_SK(cudaEventCreate(&ev0));
-  PHI_SK(cudaEventCreate(&ev1));
+  EventPair evs;
+  PHI_SK(cudaEventCreate(&evs.a));
+  PHI_SK(cudaEventCreate(&evs.b));
+  cudaEvent_t ev0 = evs.a, ev1 = evs.b;
   PHI_SK(cudaEventRecord(ev0, s));
   // b = -L(E00), element (0,0) of node 0 dropped.
   const double2 one = make_double2(1.0, 0.0);
@@ -218,8 +228,6 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     }
   }
   cudaFreeHost(host);
-  cudaEventDestroy(ev0);
-  cudaEventDestroy(ev1);
   if (result == PHI_OK || result == PHI_E_NO_CONVERGENCE) {
     const int flag = ctx->check_device_flag();
     if (flag != PHI_OK) result = flag;
