@@ -62,6 +62,7 @@ class PHI_API HierarchyIntegrator {
   void RunRkf45(std::ofstream &out);
   void RunSteadyState(std::ofstream &out);
   void WriteRestartIfAsked(double timestep);
+  void WriteMemoryLines(std::ofstream &out, long long M) const;
   void Fail(int code, const std::string &msg);
 };
 

@@ -142,10 +142,18 @@ void HierarchyIntegrator::Run(int, int, RunMethod method) {
   // PrepareForOutput (hierarchy_integrator.cc:313-319) and the t = start line
   // of InitializeDensityMatrix (:1148-1157).
   if (out.is_open()) {
+    // PhiParameters::Write, its run-method lines (phi_parameters.cc:1087-
+    // 1117) and PrepareForOutput (hierarchy_integrator.cc:313-319).
     parameters_->Write(&out, M);
-    out << "#Total Number of matrices:" << M << std::endl;
     out << "#Threads=" << parameters_->num_threads << "\n";
-    out << "#Integrator=" << (method == RK4 ? "rk4" : method == RKF45 ? "rkf45" : "bicgstab") << "\n";
+    if (!steady)
+      out << "#Integrator=" << (method == RK4 ? "rk4" : "rkf45") << "\n";
+    else if (method == BICGSTABL)
+      out << "#Calculating steady-state using BiCGSTAB(" << parameters_->bicgstab_ell << ")\n";
+    else
+      out << "#Calculating steady-state using BiCGSTAB\n";
+    out << "#Total Number of matrices:" << M << std::endl;
+    WriteMemoryLines(out, M);
     out << "#-------------\n";
     if (!steady) {
       out << parameters_->start_time << " ";
@@ -300,6 +308,31 @@ void HierarchyIntegrator::RunSteadyState(std::ofstream &out) {
   out << st.iterations << " ";
   for (int j = 0; j < N * N; ++j) out << rho[j] << " ";
   out << std::endl;
+}
+
+// Memory block of PHI's header (PrintMemoryRequirements(true),
+// hierarchy_integrator.cc:302-310), with this library's device buffers: the
+// hierarchy state, and the state plus work buffers of RK4 (y, acc and two
+// stage inputs), RKF45 (y, its ping-pong, five k, two stage inputs) and the
+// BiCGSTAB(2) steady state (x, rhat, b, r_0..r_2, u_0..u_2).  Spectra are
+// not provided (0).
+void HierarchyIntegrator::WriteMemoryLines(std::ofstream &out, long long M) const {
+  const int N = parameters_->num_states;
+  const double E = (double)N * N, EP = E + ((N * N) & 1);
+  const bool mixed = parameters_->precision == PHI_PREC_MIXED;
+  const double mb = 1.0 / 1024 / 1024;
+  const double state = 16.0 * E * M * mb, work = (mixed ? 8.0 * EP : 16.0 * E) * M * mb;
+  const float hierarchy = (float)state;
+  const float rk4 = (float)(2 * state + (mixed ? 3 : 2) * work);
+  const float rkf45 = (float)(2 * state + 7 * work + (mixed ? 2 * work : 0));
+  const float steady = (float)(state + 9 * state);
+  out << "#Memory to store matrices for calculations:\n";
+  out << "#hierarchy: " << hierarchy << " Mb.\n";
+  out << "#rk4: " << rk4 << " Mb.\n";
+  out << "#rkf45: " << rkf45 << " Mb.\n";
+  out << "#rk4spectrum: " << 0 << " Mb.\n";
+  out << "#rkf45spectrum: " << 0 << " Mb.\n";
+  out << "#steadystate: " << steady << " Mb.\n";
 }
 
 // The closing restart file of Rk4Integrate / Rkf45Integrate

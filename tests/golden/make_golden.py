@@ -12,6 +12,10 @@ Outputs (committed; the GPU host has no reference tree):
                         the problems listed in CASES (builder + arguments)
   ref_order.json        node order of the reference's ConstructI for a set of
                         (terms, truncation) pairs
+  ref_output_indep_n3_rk4.txt / .json
+                        the output file the reference's `phi` writes for an
+                        RK4 run (PrepareForOutput + dynamics rows + closing
+                        lines), for the output-file layout
   ref_restart_indep_n3.txt / .json
                         a restart file written by the reference build
                         (RestartFile, RestartOutputTimeSecs; restart_helper.cc
@@ -19,6 +23,7 @@ Outputs (committed; the GPU host has no reference tree):
                         parameters and its rho_0 printed with %.17g
 
     python tests/golden/make_golden.py /root/reference restart   # restart fixture only
+    python tests/golden/make_golden.py /root/reference output    # output-file fixture only
 """
 from __future__ import annotations
 
@@ -115,6 +120,30 @@ def make_restart_fixture():
     print("restart fixture written", flush=True)
 
 
+OUTPUT_CASE = ("random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=3), 0.001, 0.01,
+               0.002)
+
+
+def make_output_fixture():
+    builder, kw, dt, t_end, out_step = OUTPUT_CASE
+    p = build(builder, kw)
+    phi_bin = os.path.join(os.path.dirname(O.REF_DRIVER), "phi")
+    with tempfile.TemporaryDirectory() as d:
+        prm, out = os.path.join(d, "in.prm"), os.path.join(d, "out.txt")
+        with open(prm, "w") as f:
+            f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_min_step=out_step, output_file=out)
+                    .replace("verbose=-2", "verbose=0"))
+        subprocess.run([phi_bin, prm, "rk4", "1"], check=True, timeout=120, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        text = open(out).read()
+    with open(os.path.join(HERE, "ref_output_indep_n3_rk4.txt"), "w") as f:
+        f.write(text)
+    with open(os.path.join(HERE, "ref_output_indep_n3_rk4.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "builder": builder, "kwargs": kw,
+                   "method": "rk4", "timestep": dt, "t_end": t_end, "output_min_step": out_step}, f, indent=0)
+    print("output fixture written", flush=True)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
@@ -122,7 +151,11 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "restart":
         make_restart_fixture()
         return
+    if len(sys.argv) > 2 and sys.argv[2] == "output":
+        make_output_fixture()
+        return
     make_restart_fixture()
+    make_output_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)

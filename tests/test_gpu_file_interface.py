@@ -84,3 +84,45 @@ def test_cli_steady_state_output_file(tmp_path):
     rho_ref = ref.rho0(ref.steady_state())
     final = [l for l in lines if l and not l.startswith("#")][-1]
     np.testing.assert_allclose(_complexes(final), rho_ref.T.reshape(-1), rtol=1e-5, atol=1e-6)
+
+
+def test_cli_output_file_matches_reference_layout(tmp_path):
+    """Our CLI's output file against the one the reference's `phi` wrote for
+    the same parameters (tests/golden/ref_output_indep_n3_rk4.txt): the same
+    '#' header lines (memory figures are each implementation's own), the same
+    dynamics-row times and values to PHI's 6 significant digits, the same
+    closing step count and the final row to its 4 digits."""
+    import json as _json
+    here = os.path.dirname(os.path.abspath(__file__))
+    meta = _json.load(open(os.path.join(here, "golden", "ref_output_indep_n3_rk4.json")))
+    ref_lines = open(os.path.join(here, "golden", "ref_output_indep_n3_rk4.txt")).read().splitlines()
+    p = getattr(cases, meta["builder"])(**meta["kwargs"])
+    out = tmp_path / "out.txt"
+    path = _write(tmp_path, O.param_file_text(p, timestep=meta["timestep"], t_end=meta["t_end"],
+                                              output_min_step=meta["output_min_step"], output_file=str(out))
+                  .replace("verbose=-2", "verbose=0"))
+    r = subprocess.run([CLI, path, "rk4", "1"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    ours = out.read_text().splitlines()
+
+    def header(lines):
+        h = []
+        for l in lines:
+            if not l.startswith("#"):
+                break
+            key = l.split(":")[0] if (" Mb." in l) else l
+            h.append(key)
+        return h
+    assert header(ours) == header(ref_lines)
+
+    def rows(lines):
+        body = [l for l in lines if l and not l.startswith("#")]
+        return body[:-1], body[-1]
+    (ro, fo), (rr, fr) = rows(ours), rows(ref_lines)
+    assert len(ro) == len(rr)
+    for a, b in zip(ro, rr):
+        assert a.split()[0] == b.split()[0]  # the time as PHI prints it
+        np.testing.assert_allclose(_complexes(a), _complexes(b), rtol=2e-5, atol=1e-9)
+    np.testing.assert_allclose(_complexes(fo), _complexes(fr), rtol=1e-3, atol=1e-6)
+    steps = [l for l in ours if l.startswith("#Total number of integration steps")]
+    assert steps == [l for l in ref_lines if l.startswith("#Total number of integration steps")]
