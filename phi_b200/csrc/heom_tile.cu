@@ -15,7 +15,7 @@ using namespace tile_detail;
 namespace {
 
 template <int N, int KT, bool MIXED>
-__global__ void __launch_bounds__(256, TileMinBlocks<KT, MIXED>::value) heom_tile_kernel(TileParams p) {
+__global__ void __launch_bounds__(kTileThreads, TileMinBlocks<KT, MIXED>::value) heom_tile_kernel(TileParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   tile_init_barriers(smem_raw);
   tile_body<N, KT, MIXED>(p, blockIdx.x, smem_raw, 0u, 0u);
@@ -34,7 +34,7 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
     configured = (int)smem_max;
   }
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
-  kern<<<(unsigned)tiles, 256, tile_smem<N, MIXED>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
+  kern<<<(unsigned)tiles, kTileThreads, tile_smem<N, MIXED>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
   return cudaGetLastError();
 }
 

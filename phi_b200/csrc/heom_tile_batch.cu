@@ -60,10 +60,10 @@ __device__ __forceinline__ int run_tile_any(const TileParams &p, long long tile,
   }
 }
 
-constexpr int kBatchMinBlocks = 3;
+constexpr int kBatchMinBlocks = 24 / kTileWarps;  // 24 resident warps per SM
 
 template <bool MIXED>
-__global__ void __launch_bounds__(256, kBatchMinBlocks)
+__global__ void __launch_bounds__(kTileThreads, kBatchMinBlocks)
     heom_tile_batch_kernel(const TileParams *__restrict__ params, const long long *__restrict__ tile_start,
                            int count, long long total_tiles, int *err_flag) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -103,7 +103,7 @@ int tile_batch_occupancy(const TileBatchPlan &plan) {
   if (plan.smem > 48 * 1024 &&
       cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem) != cudaSuccess)
     return 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, 256, plan.smem) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, kTileThreads, plan.smem) != cudaSuccess) return 0;
   return blocks;
 }
 
@@ -117,7 +117,7 @@ cudaError_t launch_tile_batch(const TileBatchPlan &plan, int grid, cudaStream_t 
                                            (int)plan.smem);
       if (e != cudaSuccess) return e;
     }
-    heom_tile_batch_kernel<true><<<grid, 256, plan.smem, stream>>>(params, plan.tile_start, plan.count,
+    heom_tile_batch_kernel<true><<<grid, kTileThreads, plan.smem, stream>>>(params, plan.tile_start, plan.count,
                                                                  plan.total_tiles, plan.err_flag);
   } else {
     if (plan.smem > 48 * 1024) {
@@ -125,7 +125,7 @@ cudaError_t launch_tile_batch(const TileBatchPlan &plan, int grid, cudaStream_t 
                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)plan.smem);
       if (e != cudaSuccess) return e;
     }
-    heom_tile_batch_kernel<false><<<grid, 256, plan.smem, stream>>>(params, plan.tile_start, plan.count,
+    heom_tile_batch_kernel<false><<<grid, kTileThreads, plan.smem, stream>>>(params, plan.tile_start, plan.count,
                                                                   plan.total_tiles, plan.err_flag);
   }
   return cudaGetLastError();

@@ -15,7 +15,7 @@
 //          input.  complex64 buffers pad every node to an even number of
 //          elements so each node range is 16-byte aligned.
 //
-// A 256-thread CTA owns a tile of NT consecutive nodes (about one
+// A CTA of kTileThreads threads owns a tile of NT consecutive nodes (about one
 // upper-triangle pair of one node per thread).  Everything the tile reads of
 // its own nodes is contiguous in HBM and arrives by TMA bulk copies issued at
 // CTA start:
@@ -56,6 +56,8 @@
 namespace phi {
 namespace tile_detail {
 
+constexpr int kTileThreads = 256;             // threads per CTA
+constexpr int kTileWarps = kTileThreads / 32;
 constexpr int kMaxPre = 5;  // epilogue operand buffers per launch
 constexpr long long kMaxPolls = 1ll << 22;
 
@@ -153,7 +155,7 @@ struct TileShape {
   static constexpr int P = N * (N + 1) / 2;
   // About one (node, pair) item per thread; two for N >= 12, whose nodes
   // would otherwise leave a tile of one node and idle threads.
-  static constexpr int NT0 = (N >= 12 ? 512 : 256) / P;
+  static constexpr int NT0 = (N >= 12 ? 2 : 1) * kTileThreads / P;
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
   // Column stride of the derivative tile in shared memory: odd, so the
   // transposed (j, i) writes of one warp fall in distinct banks.
@@ -181,7 +183,8 @@ struct TileLayout {
 // gathered values live.
 template <int KT, bool MIXED>
 struct TileMinBlocks {
-  static constexpr int value = KT == 1 ? 5 : (KT == 2 ? (MIXED ? 5 : 4) : 3);
+  static constexpr int warps = KT == 1 ? 40 : (KT == 2 ? (MIXED ? 40 : 32) : 24);  // resident warps per SM
+  static constexpr int value = warps / kTileWarps;
 };
 
 // KT = terms per site (K + 1) under PHI's identity site map.
@@ -228,7 +231,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
   double *coef = deph + NT;                                         // 24
-  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // 8 warp maxima
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
   R *cn = reinterpret_cast<R *>(wmax + 8);                           // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
@@ -282,12 +285,12 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   const bool hreal = c.h_real;
   R *Hr = reinterpret_cast<R *>(Hs);
   if (hreal) {
-    for (int i = tid; i < E; i += 256) Hr[i] = (R)__ldg(c.H + i).x;
+    for (int i = tid; i < E; i += kTileThreads) Hr[i] = (R)__ldg(c.H + i).x;
   } else {
-    for (int i = tid; i < E; i += 256) Hs[i] = from_d2<TX>(__ldg(c.H + i));
+    for (int i = tid; i < E; i += kTileThreads) Hs[i] = from_d2<TX>(__ldg(c.H + i));
   }
-  for (int i = tid; i < E; i += 256) mats[i] = (R)__ldg(c.mats_elem + i);
-  for (int i = tid; i < P; i += 256) {
+  for (int i = tid; i < E; i += kTileThreads) mats[i] = (R)__ldg(c.mats_elem + i);
+  for (int i = tid; i < P; i += kTileThreads) {
     pi[i] = __ldg(c.pair_i + i);
     pj[i] = __ldg(c.pair_j + i);
   }
@@ -296,7 +299,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // Per (node, term): neighbour ids scaled to element offsets of the stage
   // input (-1 when absent), occupation, and the prefactor magnitudes for that
   // occupation, so the pair loop reads shared memory only.
-  for (int q = tid; q < tile_terms; q += 256) {
+  for (int q = tid; q < tile_terms; q += kTileThreads) {
     const int nd = q / T, t = q - nd * T;
     const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
     const int nt = __ldg(c.mi + n0 * T + q);
@@ -306,7 +309,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     cn[q] = (R)__ldg(c.sq_next + t * W + nt);
     cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
   }
-  for (int t = tid; t < T; t += 256) {
+  for (int t = tid; t < T; t += kTileThreads) {
     const double2 ct = __ldg(c.corr + t);
     ccr[2 * t] = (R)ct.x;
     ccr[2 * t + 1] = (R)ct.y;
@@ -328,7 +331,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // ---- phase 2: derivative of every (node, pair) ----
   const R ih = (R)c.inv_hbar;
   const int items = nt_here * P;
-  for (int it = tid; it < items; it += 256) {
+  for (int it = tid; it < items; it += kTileThreads) {
     const int nd = it / P, u = it - nd * P;
     const int i = pi[u], j = pj[u];
     const TX *X = Xs + nd * ES;
@@ -444,7 +447,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   double emax = 0.0;
   if (p.mode == kModeApply) {
     TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += 256) {
+    for (int e = tid; e < tile_elems; e += kTileThreads) {
       const int nd = e / E, w = e - nd * E;
       st_stream(out + (n0 + nd) * ES + w, Us[uix(e)]);
     }
@@ -456,7 +459,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       const Rk4Ctl *rc = p.rk4;
       if (rc->out_factor > 0 && rc->step % rc->out_factor == 0 && rc->nout < rc->capacity) row = rc->nout;
     }
-    for (int e = tid; e < tile_elems; e += 256) {
+    for (int e = tid; e < tile_elems; e += kTileThreads) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const double2 kv = to_d2(Us[uix(e)]);
@@ -486,7 +489,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     const int s = p.stage;
     const double *cf = coef;
     TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += 256) {
+    for (int e = tid; e < tile_elems; e += kTileThreads) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const TX kx = Us[uix(e)];
@@ -542,7 +545,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       if (tid == 0) {
         unsigned long long m = wmax[0];
 #pragma unroll
-        for (int w = 1; w < 8; ++w) m = wmax[w] > m ? wmax[w] : m;
+        for (int w = 1; w < kTileWarps; ++w) m = wmax[w] > m ? wmax[w] : m;
         if (m) atomicMax(&p.ctl->err_bits, m);
       }
     }
@@ -558,7 +561,7 @@ inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
   for (int i = 0; i < npre; ++i)
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
-  b += (size_t)(S::NT + 24 + 8) * sizeof(double);  // deph, coef, warp maxima
+  b += (size_t)(S::NT + 24 + kTileWarps) * sizeof(double);  // deph, coef, warp maxima
   b += (size_t)(2 * S::NT * T + 2 * T + S::E) * Lay::XB / 2;  // cn, cp, ccr, mats in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;
