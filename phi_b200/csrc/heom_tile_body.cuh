@@ -232,7 +232,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
   double *coef = deph + NT;                                         // 24
   unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
-  R *cn = reinterpret_cast<R *>(wmax + 8);                           // NT*T |next prefactor|
+  R *cn = reinterpret_cast<R *>(wmax + kTileWarps);                          // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
   R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element

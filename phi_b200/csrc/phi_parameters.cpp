@@ -497,16 +497,24 @@ void PhiParameters::Write(std::ofstream *out, long long num_matrices) {
       for (int i = 0; i < width; ++i) o << bath_coupling_op[(size_t)b * width + i] << (i + 1 < width ? "," : "\n");
     }
   }
+  // Row r as PHI prints it (phi_parameters.cc:1054-1074): elements (r, c)
+  // for c < N-1, then storage element (r+1)*N - 1 -- which is element
+  // (N-1, r), not (r, N-1); kept so the header reads back the same.
   auto matrix = [&](const char *name, const Complex *m) {
     if (!m) return;
     o << "#" << name << ":\n";
     for (int r = 0; r < num_states; ++r) {
       o << "#";
-      for (int c = 0; c < num_states; ++c)
-        o << m[r + (size_t)c * num_states] << (c + 1 < num_states ? "," : "\n");
+      for (int c = 0; c + 1 < num_states; ++c) o << m[r + (size_t)c * num_states] << ",";
+      o << m[(size_t)(r + 1) * num_states - 1] << "\n";
     }
   };
   matrix("Hamiltonian", time_indepenent_hamiltonian);
   matrix("InitialDensityMatrix", initial_density_matrix);
+  if (!restart_input_filename.empty()) o << "#RestartInput=" << restart_input_filename << "\n";
+  if (restart_output_time > 0) {
+    o << "#RestartOutputTime=" << restart_output_time << "\n";
+    o << "#RestartFile=" << restart_output_filename << "\n";
+  }
   o << "#Estimated Number of Matrices=" << num_matrices << "\n#-------------\n";
 }

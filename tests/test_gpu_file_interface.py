@@ -78,7 +78,7 @@ def test_cli_steady_state_output_file(tmp_path):
     r = subprocess.run([CLI, path, "bicgstab"], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout + r.stderr
     lines = out.read_text().splitlines()
-    assert "#Integrator=bicgstab" in lines
+    assert "#Calculating steady-state using BiCGSTAB(2)" in lines  # PhiParameters::Write (phi_parameters.cc:1108-1116)
     assert any(l.startswith("#Info: Converged to diff =") for l in lines)
     ref = O.Oracle(p)
     rho_ref = ref.rho0(ref.steady_state())
