@@ -548,7 +548,7 @@ def main():
         peak, peak_kind = peaks()
         S = M * E * 16
         EP = E + (E & 1)
-        # Algorithmic bytes of one fused RKF45 step (DESIGN.md): FP64 touches
+        # Algorithmic bytes of one fused RKF45 step: FP64 touches
         # 36 complex128 state-size arrays; mixed touches 7 complex128 (y reads,
         # y5 write) and 31 complex64 ones (stage inputs, k, y32).
         step_bytes = 36 * S if prec == capi.PHI_PREC_FP64 else M * (7 * E * 16 + 31 * EP * 8)

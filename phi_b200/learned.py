@@ -9,7 +9,7 @@ exp(-H/kT)/Z of the system Hamiltonian -- the guess PrepForSteadyState
 builds from eigen data (hierarchy_integrator.cc:1547-1588) -- which is about
 ten times smaller and smoother than rho_0 itself.  BiCGSTAB(ell)
 starts from that rho_0 with every other node zero
-(phi_gpu_steady_state_rho0); it stays the judge of the error, so a poor
+(phi_gpu_steady_state_rho0); the solver alone decides the error, so a poor
 prediction costs iterations, never accuracy.
 
 Training data are steady states the method itself produced (BiCGSTAB(2) to a
