@@ -82,6 +82,19 @@ typedef struct {
   int32_t precision;           /* PHI_PREC_* */
   int32_t device;              /* CUDA device ordinal */
   int64_t max_nodes;           /* node budget; 0 = limited by memory only */
+  double filter_tolerance;     /* filter_tolerance (FilterTolerance): > 0 turns on
+                                  adaptive hierarchy filtering for independent
+                                  baths -- after every RK4 step and every
+                                  accepted RKF45 step a node whose largest
+                                  |element| is below the tolerance stops
+                                  feeding its neighbours, and feeds them again
+                                  once it exceeds it (the DoNext / DoPrevious
+                                  overrides of IndependentBathAdaptiveTruncation,
+                                  hierarchy_updater.cc:256-303; flag updates
+                                  hierarchy_integrator.cc:2827-2850, :2359-2384).
+                                  Ignored for diagonal and full baths, as
+                                  FixIncompatibleCombinations drops it
+                                  (phi_parameters.cc:847-851).  0 = off. */
 } phi_problem_desc;
 
 typedef struct phi_ctx phi_ctx;
@@ -136,6 +149,11 @@ PHI_API int phi_gpu_get_node_table(const phi_ctx *ctx, int32_t *multi_index, int
 /* Whole-hierarchy state, host buffers of 2*M*N*N doubles. */
 PHI_API int phi_gpu_set_state(phi_ctx *ctx, const double *state);
 PHI_API int phi_gpu_get_state(const phi_ctx *ctx, double *state);
+
+/* Adaptive filtering flags of the current state, host buffer of M bytes:
+ * 1 = active (HierarchyNode::is_active).  All 1 after create, set_state,
+ * reset and restart reads, and always when filtering is off. */
+PHI_API int phi_gpu_get_active(const phi_ctx *ctx, uint8_t *flags);
 
 /* rho_0 (node 0), host buffer of 2*N*N doubles.  Replaces density_matrix()
  * (hierarchy_integrator.cc:177-191), which returns the same storage order. */

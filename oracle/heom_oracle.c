@@ -35,6 +35,8 @@ struct oracle_ctx {
   double *gamma;   /* nb */
   cplx *bath;      /* diagonal: nb*N; full: nb*N*N */
   cplx *same, *nextop, *prevop; /* diagonal / full bath operator tables */
+  double filter_tol;       /* > 0: adaptive filtering (IndependentBath only) */
+  unsigned char *active;   /* M: HierarchyNode::is_active, all 1 at the start */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -170,6 +172,9 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
   c->temp = p->temperature;
   const int T = c->T;
   c->M = oracle_node_count(T, c->trunc);
+  c->filter_tol = p->filter_tolerance;
+  c->active = (unsigned char *)malloc((size_t)(c->M > 0 ? c->M : 1));
+  if (c->active) memset(c->active, 1, (size_t)(c->M > 0 ? c->M : 1));
   if (c->M <= 0) { free(c); return NULL; }
   c->mi = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
   c->next = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
@@ -296,7 +301,7 @@ void oracle_destroy(oracle_ctx *c) {
   if (!c) return;
   free(c->mi); free(c->next); free(c->prev); free(c->tier);
   free(c->H); free(c->Hadj); free(c->corr); free(c->abs_corr); free(c->matsubara); free(c->gamma);
-  free(c->bath); free(c->same); free(c->nextop); free(c->prevop);
+  free(c->bath); free(c->same); free(c->nextop); free(c->prevop); free(c->active);
   free(c);
 }
 
@@ -397,6 +402,13 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
   const cplx *r = rho + i * E;
   cplx *d = out + i * E;
   const cplx lp = cx(0, -1.0 / c->hbar), nlp = cx(0, 1.0 / c->hbar);
+  /* Adaptive filtering (FilterTolerance, IndependentBath): PHI calls the
+   * updater through HierarchyUpdater::Get, which is not virtual
+   * (hierarchy_updater.h:36-52), so IndependentBathAdaptiveTruncation::Get
+   * (:227-240) never runs; only its virtual DoNext / DoPrevious overrides do
+   * (hierarchy_updater.cc:256-303).  So every node keeps its own terms and
+   * an inactive node contributes nothing to its neighbours. */
+  const int filtered = c->filter_tol > 0 && c->kind == ORACLE_BATH_INDEPENDENT && c->trunc > 1;
   /* DoUnitary (hierarchy_updater.h:64-70): d = -i/hbar H rho + i/hbar rho H^+. */
   for (int k = 0; k < E; ++k) d[k] = 0;
   hemm_right(N, lp, r, c->H, 0, d);
@@ -415,6 +427,26 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
         d[m * N + n] -= r[m * N + n] * (c->matsubara[n] + c->matsubara[m]);
       const int dd = (N + 1) * m;
       d[dd] += 2.0 * c->matsubara[m] * r[dd];
+    }
+    if (filtered) {  /* inactive neighbours contribute nothing */
+      int nn = 0, pp = 0;
+      for (int j = 0; j < np.num_next; ++j)
+        if (c->active[np.next_id[j]]) {
+          np.next_term[nn] = np.next_term[j];
+          np.next_id[nn] = np.next_id[j];
+          np.next_pf[nn] = np.next_pf[j];
+          ++nn;
+        }
+      for (int j = 0; j < np.num_prev; ++j)
+        if (c->active[np.prev_id[j]]) {
+          np.prev_term[pp] = np.prev_term[j];
+          np.prev_id[pp] = np.prev_id[j];
+          np.prev_row[pp] = np.prev_row[j];
+          np.prev_col[pp] = np.prev_col[j];
+          ++pp;
+        }
+      np.num_next = nn;
+      np.num_prev = pp;
     }
     /* IndependentBath::DoNext (:216-233): column m += p rho+[:, m];
      * row m -= p rho+[m, :]. */
@@ -505,6 +537,32 @@ void oracle_initial_state(const oracle_ctx *c, const double *rho0, double *state
 
 /* ------------------------------------------------------------------------ */
 
+void oracle_reset_filter(oracle_ctx *c) {
+  if (c->active) memset(c->active, 1, (size_t)c->M);
+}
+
+void oracle_get_active(const oracle_ctx *c, unsigned char *flags) {
+  memcpy(flags, c->active, (size_t)c->M);
+}
+
+/* The active flags after a state update (RK4: every step, :2827-2850;
+ * RKF45: every accepted step, :2359-2384): a node whose largest |element|
+ * falls below the tolerance is deactivated, an inactive one whose largest
+ * |element| exceeds it is reactivated. */
+static void update_filter(const oracle_ctx *c, const cplx *y) {
+  if (!(c->filter_tol > 0) || c->kind != ORACLE_BATH_INDEPENDENT || c->trunc <= 1) return;
+  const int E = c->N * c->N;
+  for (int64_t m = 0; m < c->M; ++m) {
+    double mx = 0;
+    for (int e = 0; e < E; ++e) {
+      const double a = cabs(y[m * E + e]);
+      if (a > mx) mx = a;
+    }
+    if (mx < c->filter_tol && c->active[m]) c->active[m] = 0;
+    else if (mx > c->filter_tol && !c->active[m]) c->active[m] = 1;
+  }
+}
+
 int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start_time,
                    double end_time, double output_min_step, double *traj,
                    double *traj_times, int64_t traj_capacity, int64_t *num_out) {
@@ -533,6 +591,7 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start
     apply_all(c, x, k3, temp);
     for (int64_t j = 0; j < total; ++j)                           /* :2822-2825 */
       y[j] += h6 * (k0[j] + 2.0 * k1[j] + 2.0 * k2[j] + k3[j]);
+    update_filter(c, y);                                          /* :2827-2850 */
     time_now += dt;                                               /* :2856 */
     if (output_factor > 0 && (i % output_factor) == 0) {          /* :2858 */
       if (traj && nout < traj_capacity) {
@@ -609,6 +668,7 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
     /* Accept test (:2355) taken on the step size of this attempt. */
     if (max_diff < tolerance || mydt * creal(dtdn) < min_dt) {
       memcpy(y, x, sizeof(cplx) * (size_t)total);
+      update_filter(c, y);                                        /* :2359-2384 */
       time_now += mydt;
       accepted += 1;
       int update_dt = max_diff < tolerance / 10;

@@ -44,6 +44,7 @@ typedef struct {
   const double *gamma;        /* num_baths */
   const double *lambda;       /* num_baths */
   const double *coupling;     /* diagonal: num_baths*N; full: num_baths*N*N */
+  double filter_tolerance;    /* > 0: adaptive hierarchy filtering (IndependentBath) */
 } oracle_problem;
 
 typedef struct oracle_ctx oracle_ctx;
@@ -66,8 +67,16 @@ void oracle_get_tables(const oracle_ctx *c, int32_t *multi_index, int32_t *next,
 /* c_{j,k} (2*T doubles) and the Matsubara correction Delta_j (num_baths). */
 void oracle_get_constants(const oracle_ctx *c, double *corr, double *matsubara);
 
-/* One HierarchyUpdater::Get sweep over every node (hierarchy_updater.h:36-52). */
+/* One HierarchyUpdater::Get sweep over every node (hierarchy_updater.h:36-52);
+ * with filtering, over the current active flags. */
 void oracle_apply(const oracle_ctx *c, const double *rho, double *drho);
+
+/* Adaptive filtering flags (HierarchyNode::is_active): every node active at
+ * creation and after oracle_reset_filter; oracle_rk4 / oracle_rkf45 update
+ * them after every step (accepted step) and keep them for the next call.
+ * oracle_get_active copies M bytes. */
+void oracle_reset_filter(oracle_ctx *c);
+void oracle_get_active(const oracle_ctx *c, unsigned char *flags);
 
 /* Initial hierarchy state: rho(0) scaled into node 0, zeros elsewhere
  * (hierarchy_integrator.cc:1070-1096). */

@@ -32,6 +32,7 @@ class _Problem(ctypes.Structure):
         ("hbar", c_double), ("kb", c_double), ("temperature", c_double),
         ("hamiltonian", POINTER(c_double)), ("gamma", POINTER(c_double)),
         ("lambda_", POINTER(c_double)), ("coupling", POINTER(c_double)),
+        ("filter_tolerance", c_double),
     ]
 
 
@@ -61,6 +62,8 @@ def load():
     lib.oracle_get_constants.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.oracle_apply.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.oracle_initial_state.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.oracle_reset_filter.argtypes = [c_void_p]
+    lib.oracle_get_active.argtypes = [c_void_p, c_void_p]
     lib.oracle_rk4.restype = c_int64
     lib.oracle_rk4.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
                                c_void_p, c_void_p, c_int64, POINTER(c_int64)]
@@ -135,6 +138,10 @@ class Oracle:
         elif pr.bath_kind == 2:
             v = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, n, n)
             pr.coupling = arr(np.transpose(v, (0, 2, 1)))
+        # FixIncompatibleCombinations (phi_parameters.cc:847-851): filtering
+        # only with independent baths.
+        ft = float(getattr(p, "filter_tolerance", 0.0) or 0.0)
+        pr.filter_tolerance = ft if pr.bath_kind == 0 else 0.0
         self._keep = keep
         self.ctx = self.lib.oracle_create(ctypes.byref(pr))
         if not self.ctx:
@@ -176,7 +183,21 @@ class Oracle:
         self.lib.oracle_apply(self.ctx, s.ctypes.data, out.ctypes.data)
         return out
 
-    def rk4(self, state, dt, t_end, output_min_step=0.0, capacity=0, start_time=0.0):
+    def reset_filter(self):
+        """Marks every node active (HierarchyNode::is_active)."""
+        self.lib.oracle_reset_filter(self.ctx)
+
+    def active(self):
+        """Adaptive-filtering flags of the last integrated state (M bools)."""
+        out = np.zeros(self.M, np.uint8)
+        self.lib.oracle_get_active(self.ctx, out.ctypes.data)
+        return out.astype(bool)
+
+    def rk4(self, state, dt, t_end, output_min_step=0.0, capacity=0, start_time=0.0, keep_filter=False):
+        """RK4 from `state`; the filter flags start all active (a fresh PHI
+        run) unless keep_filter continues those of the previous call."""
+        if not keep_filter:
+            self.reset_filter()
         s = np.ascontiguousarray(state, np.float64).copy()
         E2 = 2 * self.n * self.n
         traj = np.zeros(max(capacity, 1) * E2)
@@ -190,7 +211,10 @@ class Oracle:
         rows = [_from_colmajor(traj[r * E2:(r + 1) * E2], self.n) for r in range(k)]
         return s, int(steps), times[:k].copy(), np.array(rows)
 
-    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0):
+    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0, keep_filter=False):
+        """RKF45 from `state`; filter flags as for rk4."""
+        if not keep_filter:
+            self.reset_filter()
         s = np.ascontiguousarray(state, np.float64).copy()
         acc = c_int64()
         tf = c_double()
@@ -308,6 +332,9 @@ def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_to
     lines.append(f"OutputMinimumTimestep={_fmt(output_min_step if output_min_step is not None else p.output_minimum_timestep)}")
     lines.append(f"RKF45tolerance={_fmt(rkf45_tol if rkf45_tol is not None else p.rkf45_tolerance)}")
     lines.append(f"RKF45mindt={_fmt(rkf45_mindt if rkf45_mindt is not None else p.rkf45_minimum_timestep)}")
+    ft = float(getattr(p, "filter_tolerance", 0.0) or 0.0)
+    if ft > 0:
+        lines.append(f"FilterTolerance={_fmt(ft)}")
     return "\n".join(lines) + "\n"
 
 

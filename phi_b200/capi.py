@@ -62,6 +62,7 @@ class PhiProblemDesc(ctypes.Structure):
         ("precision", c_int32),
         ("device", c_int32),
         ("max_nodes", c_int64),
+        ("filter_tolerance", c_double),
     ]
 
 
@@ -111,6 +112,7 @@ SIGNATURES = [
     ("phi_gpu_set_state", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_state", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_rho0", c_int, [c_void_p, c_void_p]),
+    ("phi_gpu_get_active", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_apply", c_int, [c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_apply_device", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_rk4", c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_void_p, c_int64,

@@ -52,6 +52,11 @@ struct HeomConsts {
   const uint8_t *pair_i;     // N(N+1)/2 upper-triangle pairs (i <= j)
   const uint8_t *pair_j;
   int *err_flag;             // set by a kernel whose bounded wait gave up
+  // Adaptive hierarchy filtering (PHI's FilterTolerance, independent baths):
+  // a node whose largest |element| drops below filter_tol stops feeding its
+  // neighbours until it rises above it again.
+  int filtered;
+  double filter_tol;
 };
 
 // Device control block of the adaptive integrator; lives in device memory and

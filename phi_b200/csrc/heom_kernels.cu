@@ -71,8 +71,9 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int T, int kind) {
   p.E = N * N;
   p.gcols = kind == kIndependent ? 2 * T * N : 2 * N * N;
   p.per_group = 3 * p.E + p.gcols;
-  // ids[2T], nts[T], then one double at an even int offset.
-  p.ints_per_group = ((3 * T + 1) & ~1) + 2;
+  // ids[2T], nts[T], then two 8-byte slots at an even int offset (the
+  // node's dephasing rate and, when filtering, its max |y|^2).
+  p.ints_per_group = ((3 * T + 1) & ~1) + 4;
   return p;
 }
 
@@ -93,6 +94,9 @@ struct StageParams {
   double2 *k[5];
   double2 *ybuf[2];
   Rkf45Ctl *ctl;
+  // filtering (see StageLaunch)
+  uint8_t *act[2];
+  int act_par;
 };
 
 template <int GROUP, int KIND>
@@ -113,6 +117,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
   int *ids = reinterpret_cast<int *>(coef_s + 32) + (size_t)g * plan.ints_per_group;
   int *nts = ids + 2 * T;
   double *deph_s = reinterpret_cast<double *>(ids + ((3 * T + 1) & ~1));  // 8-byte aligned
+  unsigned long long *nmax_s = reinterpret_cast<unsigned long long *>(deph_s + 1);
 
   int ycur = 0;
   if (p.mode == kModeRkf45) {
@@ -128,11 +133,25 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
   // RKF45 stage 0 reads the current state, whose buffer only the device knows.
   const double2 *xin = (p.mode == kModeRkf45 && p.stage == 0) ? p.ybuf[ycur] : p.x;
   const double2 *yin = p.mode == kModeRkf45 ? p.ybuf[ycur] : p.y;
+  // Filtering: flags of the current state, and of the state this launch
+  // writes (RK4 stage 3, RKF45 stage 5 -- the candidate, kept on accept).
+  const uint8_t *act_in = nullptr;
+  uint8_t *act_out = nullptr;
+  if (c.filtered) {
+    const int ap = p.mode == kModeRkf45 ? ycur : p.act_par;
+    act_in = p.act[ap];
+    act_out = p.act[ap ^ 1];
+  }
+  const bool flag_stage = act_in && act_out &&
+                          ((p.mode == kModeRk4 && p.stage == 3) || (p.mode == kModeRkf45 && p.stage == 5));
 
   for (long long n = (long long)blockIdx.x * NG + g; n < c.M; n += (long long)gridDim.x * NG) {
     // 1. metadata
-    for (int s = lane; s < 2 * T; s += GROUP)
-      ids[s] = s < T ? __ldg(c.next + n * T + s) : __ldg(c.prev + n * T + (s - T));
+    for (int s = lane; s < 2 * T; s += GROUP) {
+      const int id = s < T ? __ldg(c.next + n * T + s) : __ldg(c.prev + n * T + (s - T));
+      // an inactive neighbour contributes nothing (hierarchy_updater.cc:256-303)
+      ids[s] = (id >= 0 && act_in && !__ldg(act_in + id)) ? -1 : id;
+    }
     for (int t = lane; t < T; t += GROUP) nts[t] = __ldg(c.mi + n * T + t);
     // 2. own ADO
     const double2 *xn = xin + n * E;
@@ -142,6 +161,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
       double d = 0.0;
       for (int t = 0; t < T; ++t) d += nts[t] * __ldg(c.nu + t);
       deph_s[0] = d;
+      nmax_s[0] = 0ull;
     }
     if (KIND == kIndependent && !c.vacuum) {
       for (int idx = lane; idx < 2 * T * N; idx += GROUP) {
@@ -327,6 +347,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
 
     // 5. epilogue
     const long long base = n * E;
+    double fl_m = 0.0;  // filtering: max |y_new|^2 of this lane's elements
     if (p.mode == kModeApply) {
       for (int e = lane; e < E; e += GROUP) p.out[base + e] = Us[e];
     } else if (p.mode == kModeRk4) {
@@ -344,6 +365,8 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
         } else {
           const double2 yn = c_axpy(p.acc[base + e], kv, p.w_acc);
           p.y[base + e] = yn;
+          const double m2 = fma(yn.x, yn.x, yn.y * yn.y);
+          fl_m = m2 > fl_m ? m2 : fl_m;
           if (n == 0 && p.traj) Xs[e] = yn;
         }
       }
@@ -389,9 +412,23 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
           y5 = c_axpy(y5, k4, cf[22]);
           y5 = c_axpy(y5, kv, cf[23]);
           p.ybuf[ycur ^ 1][base + e] = y5;
+          const double m2 = fma(y5.x, y5.x, y5.y * y5.y);
+          fl_m = m2 > fl_m ? m2 : fl_m;
           const double err = hypot(y4.x - y5.x, y4.y - y5.y);
           emax = (err > emax || err != err) ? err : emax;
         }
+      }
+    }
+    if (flag_stage) {
+      // New flags of the state just written (hierarchy_integrator.cc:2827-2850,
+      // :2359-2384): below the tolerance -> inactive, above -> active, equal
+      // -> unchanged.  A NaN never wins the `>` above, as in PHI's scan.
+      if (fl_m > 0.0) atomicMax(nmax_s, (unsigned long long)__double_as_longlong(fl_m));
+      group_sync<GROUP>(g);
+      if (lane == 0) {
+        const double mx = sqrt(__longlong_as_double((long long)nmax_s[0]));
+        const uint8_t old = act_in[n];
+        act_out[n] = mx < c.filter_tol ? (uint8_t)0 : (mx > c.filter_tol ? (uint8_t)1 : old);
       }
     }
     group_sync<GROUP>(g);
@@ -527,6 +564,9 @@ cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream) {
   p.ybuf[0] = L.ybuf[0];
   p.ybuf[1] = L.ybuf[1];
   p.ctl = L.ctl;
+  p.act[0] = L.act[0];
+  p.act[1] = L.act[1];
+  p.act_par = L.act_par;
   const size_t smem = stage_smem_bytes(L.c.N, L.c.T, L.c.kind);
   const int grid = L.grid;
   const int group = choose_group(L.c.N);

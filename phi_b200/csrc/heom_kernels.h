@@ -26,6 +26,11 @@ struct StageLaunch {
   double2 *k[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // RKF45 k0..k4
   double2 *ybuf[2] = {nullptr, nullptr};                          // RKF45 state ping-pong
   Rkf45Ctl *ctl = nullptr;
+  // Filtering (c.filtered): active flags of the current state in
+  // act[act_par] (RKF45: act[ycur], chosen on the device); the stage that
+  // writes the new state writes its flags to the other buffer.
+  uint8_t *act[2] = {nullptr, nullptr};
+  int act_par = 0;
   // Tiled kernel: stage input / output and k buffers in the context's
   // storage type (complex128, or complex64 in mixed precision), the
   // complex64 copies of the state, and the arithmetic.

@@ -105,6 +105,9 @@ TileParams tile_params_for(const StageLaunch &L) {
   p.y32buf[0] = L.y32buf[0];
   p.y32buf[1] = L.y32buf[1];
   p.ctl = L.ctl;
+  p.act[0] = L.act[0];
+  p.act[1] = L.act[1];
+  p.act_par = L.act_par;
   const bool mixed = L.mixed;
   const int xb = mixed ? 8 : 16;
   // Epilogue operands of this (mode, stage), in the order the epilogue reads them.

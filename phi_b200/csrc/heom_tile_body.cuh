@@ -78,6 +78,8 @@ struct TileParams {
   double2 *ybuf[2];     // RKF45 state ping-pong
   void *y32buf[2];      // MIXED RKF45: complex64 copies of ybuf
   Rkf45Ctl *ctl;
+  uint8_t *act[2];               // filtering: active flags (see StageLaunch)
+  int act_par;
   int npre;                      // epilogue operands prefetched
   const void *pre[kMaxPre];      // sources; slot 0 of RKF45 is chosen on the device
   int pre_bytes[kMaxPre];        // 16 (complex128) or 8 (complex64)
@@ -187,6 +189,33 @@ struct TileMinBlocks {
   static constexpr int value = warps / kTileWarps;
 };
 
+// New filter flags of a tile's nodes from |y_new|^2 staged in the first 8
+// bytes of each derivative-tile slot (slot bytes apart, column stride NP):
+// one warp per node; below the tolerance -> inactive, above -> active, equal
+// -> unchanged (hierarchy_integrator.cc:2827-2850, :2359-2384).  A NaN never
+// wins the `>`, as in PHI's scan.  Kept out of line so its registers do not
+// add to the tile body's.
+static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, int slot, int N, int NP, int nt_here,
+                                               const uint8_t *act_in, uint8_t *act_out, double tol) {
+  const int E = N * N, lane = threadIdx.x & 31;
+  for (int nd = threadIdx.x >> 5; nd < nt_here; nd += kTileWarps) {
+    double m = 0.0;
+    for (int w = lane; w < E; w += 32) {
+      const int col = w / N;
+      const double v = *reinterpret_cast<const double *>(us + (size_t)(nd * N * NP + (w - col * N) + col * NP) * slot);
+      m = v > m ? v : m;
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_xor_sync(0xffffffffu, m, off);
+      m = o > m ? o : m;
+    }
+    if (lane == 0) {
+      const double mx = sqrt(m);
+      act_out[nd] = mx < tol ? (uint8_t)0 : (mx > tol ? (uint8_t)1 : act_in[nd]);
+    }
+  }
+}
+
 // KT = terms per site (K + 1) under PHI's identity site map.
 // One tile (NT consecutive nodes of one hierarchy) of one stage.  The caller
 // has initialised the two mbarriers at the start of shared memory and passes
@@ -250,6 +279,15 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   }
   const long long n0 = tile * NT;
   if (n0 >= c.M) return 1;
+  // Filtering: the flags of the current state are p.act[ap], ap = ycur
+  // (RKF45) or p.act_par; the launch that writes the new state (RK4 stage 3,
+  // RKF45 stage 5 -- the candidate, kept on accept) writes its flags to
+  // p.act[ap ^ 1].  Both are recomputed from the parameters where used, so
+  // nothing of it stays live across the tile.
+  auto flag_stage = [&]() {
+    return c.filtered && ((p.mode == kModeRk4 && p.stage == 3) || (p.mode == kModeRkf45 && p.stage == 5));
+  };
+  auto act_idx = [&]() { return p.mode == kModeRkf45 ? ycur : p.act_par; };
   const int nt_here = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
   const TX *xin;
   if (p.mode == kModeRkf45 && p.stage == 0)
@@ -299,12 +337,17 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // Per (node, term): neighbour ids scaled to element offsets of the stage
   // input (-1 when absent), occupation, and the prefactor magnitudes for that
   // occupation, so the pair loop reads shared memory only.
+  const uint8_t *act_in = c.filtered ? p.act[act_idx()] : nullptr;
   for (int q = tid; q < tile_terms; q += kTileThreads) {
     const int nd = q / T, t = q - nd * T;
     const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
     const int nt = __ldg(c.mi + n0 * T + q);
-    ids[nd * 2 * T + t] = nx >= 0 ? nx * ES : -1;
-    ids[nd * 2 * T + T + t] = pv >= 0 ? pv * ES : -1;
+    // An inactive neighbour contributes nothing (the DoNext / DoPrevious
+    // overrides of IndependentBathAdaptiveTruncation, hierarchy_updater.cc:256-303).
+    const bool nx_on = nx >= 0 && (!act_in || __ldg(act_in + nx));
+    const bool pv_on = pv >= 0 && (!act_in || __ldg(act_in + pv));
+    ids[nd * 2 * T + t] = nx_on ? nx * ES : -1;
+    ids[nd * 2 * T + T + t] = pv_on ? pv * ES : -1;
     nts[q] = nt;
     cn[q] = (R)__ldg(c.sq_next + t * W + nt);
     cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
@@ -445,6 +488,12 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   auto preD = [&](int b) { return reinterpret_cast<const double2 *>(PreBase + pre_off[b]); };
   auto preX = [&](int b) { return reinterpret_cast<const TX *>(PreBase + pre_off[b]); };
   double emax = 0.0;
+  // Filtering: |y_new|^2 of element e goes to the first 8 bytes of its own
+  // slot Us[uix(e)], which only this thread reads, and only before; the
+  // per-node maxima are taken from there after the loop.
+  auto fl_put = [&](int e, double2 v) {
+    *reinterpret_cast<double *>(&Us[uix(e)]) = fma(v.x, v.x, v.y * v.y);
+  };
   if (p.mode == kModeApply) {
     TX *out = static_cast<TX *>(p.out);
     for (int e = tid; e < tile_elems; e += kTileThreads) {
@@ -475,6 +524,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         p.y[gd] = yn;
         if (MIXED) static_cast<TX *>(p.y32)[gx] = from_d2<TX>(yn);
         if (row >= 0 && e < E) p.traj[row * E + e] = yn;
+        if (flag_stage()) fl_put(e, yn);
       }
     }
     if (s == 3 && n0 == 0 && p.traj) {
@@ -519,6 +569,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         y5 = cfma(y5, kv, cf[23]);
         st_stream(p.ybuf[ycur ^ 1] + gd, y5);
         if (MIXED) st_stream(static_cast<TX *>(p.y32buf[ycur ^ 1]) + gx, from_d2<TX>(y5));
+        if (flag_stage()) fl_put(e, y5);
         const double dx = y4.x - y5.x, dy = y4.y - y5.y;
         if (MIXED) {
           // max of |y4 - y5|^2; one square root per thread below
@@ -549,6 +600,15 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         if (m) atomicMax(&p.ctl->err_bits, m);
       }
     }
+  }
+  if (flag_stage()) {
+    // New flags of the state just written (hierarchy_integrator.cc:2827-2850,
+    // :2359-2384): below the tolerance -> inactive, above -> active, equal ->
+    // unchanged.
+    __syncthreads();
+    const int ap = act_idx();
+    tile_filter_flags(reinterpret_cast<const unsigned char *>(Us), (int)sizeof(TX), N, NP, nt_here,
+                      p.act[ap] + n0, p.act[ap ^ 1] + n0, c.filter_tol);
   }
   return 0;
 }

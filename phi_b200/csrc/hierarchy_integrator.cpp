@@ -27,7 +27,6 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
     return reject("Hilbert-space truncation is outside this library's scope");
   if (p.use_time_local_truncation) return reject("time-local truncation is outside this library's scope");
-  if (p.filter_tolerance > 0) return reject("adaptive hierarchy filtering is outside this library's scope");
   if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
   const bool steady = p.run_method == BICGSTAB || p.run_method == BICGSTABL || p.run_method == BICGSTABU;
   if (p.initial_density_matrix == nullptr && !steady && !p.is_restarted)
@@ -62,6 +61,7 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   d->precision = p.precision;
   d->device = p.device;
   d->max_nodes = 0;
+  d->filter_tolerance = p.filter_tolerance;  // already 0 for diagonal / full baths
   return PHI_OK;
 }
 

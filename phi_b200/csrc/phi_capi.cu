@@ -227,6 +227,10 @@ int setup_constants(phi_ctx *ctx) {
   c.pair_i = cb.pair_i.as<uint8_t>();
   c.pair_j = cb.pair_j.as<uint8_t>();
   c.err_flag = cb.err_flag.as<int>();
+  // FixIncompatibleCombinations keeps filtering for independent baths only
+  // (phi_parameters.cc:847-851); a single tier has no neighbours to filter.
+  c.filtered = (d.bath_kind == PHI_BATH_INDEPENDENT && d.filter_tolerance > 0 && !vacuum) ? 1 : 0;
+  c.filter_tol = c.filtered ? d.filter_tolerance : 0.0;
   return PHI_OK;
 }
 
@@ -275,6 +279,8 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (!is_hermitian(d.initial_density_matrix, N, nullptr))
     return fail(nullptr, PHI_E_INVALID,
                 "initial density matrix is not Hermitian (PHI's hierarchy keeps every ADO Hermitian)");
+  if (!(d.filter_tolerance >= 0) || !std::isfinite(d.filter_tolerance))
+    return fail(nullptr, PHI_E_INVALID, "filter_tolerance must be finite and >= 0");
 
   std::unique_ptr<phi_ctx> ctx(new phi_ctx());
   ctx->desc = d;
@@ -344,6 +350,11 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
                         cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && ctx->c.filtered) {
+    if (ctx->active[0].alloc((size_t)ctx->hier.M) != cudaSuccess || ctx->active[1].alloc((size_t)ctx->hier.M) != cudaSuccess)
+      return fail(nullptr, PHI_E_OOM, "filter flag allocation failed");
+    e = ctx->reset_filter();
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("initial state: ") + cudaGetErrorString(e));
   ctx->time = 0.0;
@@ -387,9 +398,34 @@ extern "C" int phi_gpu_get_node_table(const phi_ctx *cctx, int32_t *multi_index,
   return PHI_OK;
 }
 
+cudaError_t phi_ctx::reset_filter() {
+  if (!c.filtered) return cudaSuccess;
+  return cudaMemsetAsync(active[0].ptr, 1, (size_t)hier.M, stream);
+}
+
+void phi_ctx::bind_filter(phi::StageLaunch &L, int par) const {
+  if (!c.filtered) return;
+  L.act[0] = static_cast<uint8_t *>(active[0].ptr);
+  L.act[1] = static_cast<uint8_t *>(active[1].ptr);
+  L.act_par = par;
+}
+
+extern "C" int phi_gpu_get_active(const phi_ctx *cctx, uint8_t *flags) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !flags) return PHI_E_INVALID;
+  if (!ctx->c.filtered) {
+    std::memset(flags, 1, (size_t)ctx->hier.M);
+    return PHI_OK;
+  }
+  PHI_CUDA(ctx, cudaMemcpyAsync(flags, ctx->active[0].ptr, (size_t)ctx->hier.M, cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
 extern "C" int phi_gpu_set_state(phi_ctx *ctx, const double *state) {
   if (!ctx || !state) return PHI_E_INVALID;
   PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, state, ctx->state_bytes(), cudaMemcpyHostToDevice, ctx->stream));
+  PHI_CUDA(ctx, ctx->reset_filter());
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PHI_OK;
 }
@@ -439,6 +475,7 @@ extern "C" int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out,
   L.xv = d_in;
   L.outv = d_out;
   L.mixed = ctx->mixed();
+  ctx->bind_filter(L, 0);
   PHI_CUDA(ctx, phi::launch_stage(L, static_cast<cudaStream_t>(stream)));
   return PHI_OK;
 }
@@ -481,6 +518,7 @@ extern "C" int phi_gpu_reset(phi_ctx *ctx, double time) {
   PHI_CUDA(ctx, cudaMemsetAsync(ctx->y.ptr, 0, ctx->state_bytes(), ctx->stream));
   PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
                                 cudaMemcpyHostToDevice, ctx->stream));
+  PHI_CUDA(ctx, ctx->reset_filter());
   ctx->time = time;
   ctx->rkf45_started = false;
   return PHI_OK;

@@ -10,6 +10,7 @@
 #include "../../include/phi_b200.h"
 #include "heom_device.cuh"
 #include "heom_internal.h"
+#include "heom_kernels.h"
 
 // Device copies of the per-term / per-element constants (HeomConsts points here).
 struct PhiConstBuffers {
@@ -46,6 +47,9 @@ struct phi_ctx {
   phi::DeviceBuffer kbuf[5];   // RKF45 k0..k4
   phi::DeviceBuffer ctl;       // Rkf45Ctl / Rk4Ctl
   phi::DeviceBuffer traj;      // rho_0 rows
+  // Filtering (c.filtered): active flags, M bytes each.  Between calls the
+  // flags of the current state are in active[0].
+  phi::DeviceBuffer active[2];
   int work_level = 0;          // 1: xa/xb, 2: + acc, 3: + RKF45 buffers
 
   // Captured step graphs.
@@ -87,6 +91,10 @@ struct phi_ctx {
   void release_graphs();
   // PHI_E_TIMEOUT if a kernel's bounded wait gave up since the last check.
   int check_device_flag();
+  // Marks every node active (a newly set state), enqueued on `stream`.
+  cudaError_t reset_filter();
+  // Points a stage launch at the flag buffers (no-op when filtering is off).
+  void bind_filter(phi::StageLaunch &L, int par) const;
 };
 
 namespace phi {

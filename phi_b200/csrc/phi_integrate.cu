@@ -84,10 +84,12 @@ void phi_ctx::release_graphs() {
 
 namespace {
 
-// Enqueues one RK4 step (four fused stage kernels).
-cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, cudaStream_t s) {
+// Enqueues one RK4 step (four fused stage kernels).  With filtering the step
+// reads the flags in active[par] and its last stage writes active[par ^ 1].
+cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, int par, cudaStream_t s) {
   phi::StageLaunch L;
   L.c = ctx->c;
+  ctx->bind_filter(L, par);
   L.mode = phi::kModeRk4;
   L.grid = ctx->grid;
   L.y = ctx->y.as<double2>();
@@ -123,6 +125,7 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
   L.mode = phi::kModeRkf45;
   L.grid = ctx->grid;
   L.ctl = ctx->ctl.as<phi::Rkf45Ctl>();
+  ctx->bind_filter(L, 0);  // the kernels index the flags by ycur
   L.ybuf[0] = ctx->y.as<double2>();
   L.ybuf[1] = ctx->y_alt.as<double2>();
   L.mixed = ctx->mixed();
@@ -217,8 +220,8 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
     if (ctx->rk4_graph) cudaGraphExecDestroy(ctx->rk4_graph);
     ctx->rk4_graph = nullptr;
     PHI_CK(capture(ctx->stream, [&]() {
-      for (int i = 0; i < kGraphSteps; ++i) {
-        cudaError_t e = enqueue_rk4_step(ctx, dt, dtraj, ctx->stream);
+      for (int i = 0; i < kGraphSteps; ++i) {  // kGraphSteps is even: flag parity i & 1
+        cudaError_t e = enqueue_rk4_step(ctx, dt, dtraj, i & 1, ctx->stream);
         if (e != cudaSuccess) return e;
       }
       return cudaSuccess;
@@ -231,7 +234,10 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
     PHI_CK(cudaGraphLaunch(ctx->rk4_graph, ctx->stream));
     done += kGraphSteps;
   }
-  for (; done < steps; ++done) PHI_CK(enqueue_rk4_step(ctx, dt, dtraj, ctx->stream));
+  for (; done < steps; ++done) PHI_CK(enqueue_rk4_step(ctx, dt, dtraj, (int)(done & 1), ctx->stream));
+  if (ctx->c.filtered && (steps & 1))  // the current flags back in active[0]
+    PHI_CK(cudaMemcpyAsync(ctx->active[0].ptr, ctx->active[1].ptr, (size_t)ctx->hier.M,
+                           cudaMemcpyDeviceToDevice, ctx->stream));
   if (rows > 0) {
     PHI_CK(cudaMemcpyAsync(traj, dtraj, (size_t)rows * ctx->desc.num_states * ctx->desc.num_states * sizeof(double2),
                            cudaMemcpyDeviceToHost, ctx->stream));
@@ -329,6 +335,7 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
     if (hc.ycur == 1) {
       std::swap(ctx->y, ctx->y_alt);
       std::swap(ctx->y32, ctx->y32_alt);
+      std::swap(ctx->active[0], ctx->active[1]);
       ctx->release_graphs();  // captured graphs bake in the y / y_alt pointers
     }
     ctx->time = hc.time;

@@ -100,6 +100,7 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
     L.c = ctx->c;
     L.mode = phi::kModeRk4;
     L.grid = ctx->grid;
+    ctx->bind_filter(L, 0);
     const double a[4] = {dt / 2, dt / 2, dt, 0.0};
     const double w[4] = {dt / 6, dt / 3, dt / 3, dt / 6};
     const double2 *in[4] = {y, xa, xb, xa};
@@ -114,6 +115,11 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
       L.w_acc = w[st];
       e = phi::launch_stage(L, static_cast<cudaStream_t>(stream));
     }
+    // Filtering: the step wrote the new flags to active[1]; the current ones
+    // live in active[0] between calls (a device copy, no allocation).
+    if (e == cudaSuccess && ctx->c.filtered)
+      e = cudaMemcpyAsync(ctx->active[0].ptr, ctx->active[1].ptr, (size_t)ctx->hier.M,
+                          cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
   }
   if (prev_device != device) cudaSetDevice(prev_device);
   if (e != cudaSuccess) {

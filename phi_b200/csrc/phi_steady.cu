@@ -38,6 +38,7 @@ cudaError_t apply_fp64(phi_ctx *ctx, const double2 *in, double2 *out, cudaStream
   L.xv = in;
   L.outv = out;
   L.mixed = false;
+  ctx->bind_filter(L, 0);  // all active unless a filtered integration ran before
   return phi::launch_stage(L, s);
 }
 

@@ -50,6 +50,7 @@ class PhiParameters:
     rkf45_tolerance: float = 1e-6
     rkf45_minimum_timestep: float = 1e-6
     bicgstab_tolerance: float = 1e-6
+    filter_tolerance: float = 0.0
 
     @property
     def bath_kind(self) -> int:
@@ -132,6 +133,7 @@ def problem_desc(p: PhiParameters, precision: int, device: int, max_nodes: int, 
     d.precision = precision
     d.device = device
     d.max_nodes = max_nodes
+    d.filter_tolerance = float(p.filter_tolerance or 0.0)
     return d
 
 
@@ -228,6 +230,13 @@ class Hierarchy:
         s = np.ascontiguousarray(state, dtype=np.float64)
         assert s.size == self.state_len
         self._check(self.lib.phi_gpu_set_state(self.ctx, s.ctypes.data))
+
+    def active(self) -> np.ndarray:
+        """Adaptive-filtering flags of the current state (M bools; all True
+        when filtering is off)."""
+        out = np.zeros(self.num_nodes, np.uint8)
+        self._check(self.lib.phi_gpu_get_active(self.ctx, out.ctypes.data))
+        return out.astype(bool)
 
     def rho0(self) -> np.ndarray:
         out = np.zeros(2 * self.n * self.n, np.float64)

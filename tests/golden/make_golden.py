@@ -22,8 +22,15 @@ Outputs (committed; the GPU host has no reference tree):
                         :30-53) at the end of an RK4 run, with the run's
                         parameters and its rho_0 printed with %.17g
 
+  ref_filter.json       adaptive hierarchy filtering (FilterTolerance): per
+                        case, rho_0 printed with %.17g by the reference
+                        build and, for hierarchies of at most 100 nodes, the
+                        whole final state from the restart file the same run
+                        wrote (PHI prints it with 6 significant digits)
+
     python tests/golden/make_golden.py /root/reference restart   # restart fixture only
     python tests/golden/make_golden.py /root/reference output    # output-file fixture only
+    python tests/golden/make_golden.py /root/reference filter    # filtering fixture only
 """
 from __future__ import annotations
 
@@ -144,6 +151,59 @@ def make_output_fixture():
     print("output fixture written", flush=True)
 
 
+# (case id, builder, builder kwargs, method, timestep, t_end, FilterTolerance)
+FILTER_CASES = [
+    ("rand_n3_k2_t4/rk4/1e-3", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=4, seed=2), "rk4", 0.001, 0.05, 1e-3),
+    ("rand_n3_k2_t4/rkf45/1e-3", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=4, seed=2), "rkf45", 0.001, 0.05, 1e-3),
+    ("rand_n4_k1_t5/rk4/1e-2", "random_problem",
+     dict(kind="independent", n=4, matsubara=1, truncation=5, seed=1), "rk4", 0.001, 0.05, 1e-2),
+    ("rand_n3_k2_t5/rkf45/1e-4", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=5, seed=2), "rkf45", 0.001, 0.1, 1e-4),
+    ("frenkel7_L3/rk4/1e-3", "config:frenkel7", dict(depth=3), "rk4", 0.001, 0.05, 1e-3),
+]
+
+
+def parse_restart_state(text: str, n: int) -> list:
+    """Every "(re,im)" of a PHI restart file after its time and dt lines, in
+    file order (node-major, column-major within a node)."""
+    body = text.split("\n", 2)[2]
+    return [[float(a), float(b)] for a, b in re.findall(r"\(([^,()]+),([^,()]+)\)", body)]
+
+
+def make_filter_fixture():
+    outs = []
+    for cid, builder, kw, method, dt, t_end, ft in FILTER_CASES:
+        p = build(builder, kw)
+        p.filter_tolerance = ft
+        if method == "rkf45":
+            p.fix_incompatible_combinations("rkf45")
+        with tempfile.TemporaryDirectory() as d:
+            prm, out, rst, rho_f = (os.path.join(d, x) for x in ("in.prm", "out.txt", "restart.txt", "rho.txt"))
+            with open(prm, "w") as f:
+                f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_file=out)
+                        + f"RestartFile={rst}\nRestartOutputTimeSecs=1\n")
+            try:
+                subprocess.run([O.REF_DRIVER, "run", prm, method, "1", rho_f], check=True, timeout=120,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            except subprocess.TimeoutExpired:
+                print(f"{cid}: TIMEOUT", flush=True)
+                continue
+            rho = O.parse_rho_file(rho_f, p.num_states)
+            state = parse_restart_state(open(rst).read(), p.num_states)
+        M = len(state) // (p.num_states * p.num_states)
+        case = {"id": cid, "builder": builder, "kwargs": kw, "method": method, "timestep": dt, "t_end": t_end,
+                "filter_tolerance": ft, "num_nodes": M,
+                "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}
+        if M <= 100:
+            case["state_6_digits"] = state
+        outs.append(case)
+        print(f"{cid}: M={M}", flush=True)
+    with open(os.path.join(HERE, "ref_filter.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
@@ -154,8 +214,12 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "output":
         make_output_fixture()
         return
+    if len(sys.argv) > 2 and sys.argv[2] == "filter":
+        make_filter_fixture()
+        return
     make_restart_fixture()
     make_output_fixture()
+    make_filter_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)

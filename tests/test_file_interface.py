@@ -25,8 +25,7 @@ def test_unknown_method_is_rejected(tmp_path):
         Hierarchy.from_file(_write(tmp_path, text), "no_such_method")
 
 
-@pytest.mark.parametrize("line", ["FilterTolerance=1e-6", "TimeLocal=1"],
-                         ids=["filtering", "time_local"])
+@pytest.mark.parametrize("line", ["TimeLocal=1"], ids=["time_local"])
 def test_out_of_scope_features_are_rejected(tmp_path, line):
     text = O.param_file_text(configs.frenkel7(depth=2)) + line + "\n"
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
