@@ -37,6 +37,13 @@ struct oracle_ctx {
   cplx *same, *nextop, *prevop; /* diagonal / full bath operator tables */
   double filter_tol;       /* > 0: adaptive filtering (IndependentBath only) */
   unsigned char *active;   /* M: HierarchyNode::is_active, all 1 at the start */
+  /* Time-local truncation (IndependentBath): per bath m and term k the
+   * matrix Q_{m,k} (time_local_truncation_terms_th_), the sum Q_m and its
+   * adjoint (time_local_matrices_ / _adjoint_), and the stored copies
+   * (time_local_truncation_store_th_, time_local_matrices_store_). */
+  int tl;
+  cplx *tlqk, *tlqk_st;    /* nb*K1*N*N */
+  cplx *tlq, *tlq_st, *tlqa;  /* nb*N*N */
 };
 
 /* ------------------------------------------------------------------------ */
@@ -173,6 +180,7 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
   const int T = c->T;
   c->M = oracle_node_count(T, c->trunc);
   c->filter_tol = p->filter_tolerance;
+  c->tl = p->time_local && p->bath_kind == ORACLE_BATH_INDEPENDENT;
   c->active = (unsigned char *)malloc((size_t)(c->M > 0 ? c->M : 1));
   if (c->active) memset(c->active, 1, (size_t)(c->M > 0 ? c->M : 1));
   if (c->M <= 0) { free(c); return NULL; }
@@ -180,6 +188,14 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
   c->next = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
   c->prev = (int32_t *)malloc(sizeof(int32_t) * (size_t)(c->M * T + 1));
   c->tier = (int32_t *)malloc(sizeof(int32_t) * (size_t)c->M);
+  if (c->tl) {  /* zeroed, as SetElementsToZero does (hierarchy_integrator.cc:954-980) */
+    const size_t E = (size_t)c->N * c->N, nq = (size_t)c->nb * E;
+    c->tlqk = (cplx *)calloc(nq * (size_t)c->K1, sizeof(cplx));
+    c->tlqk_st = (cplx *)calloc(nq * (size_t)c->K1, sizeof(cplx));
+    c->tlq = (cplx *)calloc(nq, sizeof(cplx));
+    c->tlq_st = (cplx *)calloc(nq, sizeof(cplx));
+    c->tlqa = (cplx *)calloc(nq, sizeof(cplx));
+  }
   if (oracle_build_hierarchy(T, c->trunc, c->mi, c->M) != c->M) {
     oracle_destroy(c);
     return NULL;
@@ -302,6 +318,7 @@ void oracle_destroy(oracle_ctx *c) {
   free(c->mi); free(c->next); free(c->prev); free(c->tier);
   free(c->H); free(c->Hadj); free(c->corr); free(c->abs_corr); free(c->matsubara); free(c->gamma);
   free(c->bath); free(c->same); free(c->nextop); free(c->prevop); free(c->active);
+  free(c->tlqk); free(c->tlqk_st); free(c->tlq); free(c->tlq_st); free(c->tlqa);
   free(c);
 }
 
@@ -413,7 +430,10 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
   for (int k = 0; k < E; ++k) d[k] = 0;
   hemm_right(N, lp, r, c->H, 0, d);
   hemm_left(N, nlp, r, c->Hadj, 1, d);
-  if (c->trunc == 1) return; /* Vacuum updater: unitary part only (:206-219). */
+  /* Vacuum updater: unitary part only (:206-219).  With time-local
+   * truncation a single tier runs NoHierarchyIndependentBath through the
+   * base Get instead (hierarchy_integrator.cc:1741-1758). */
+  if (c->trunc == 1 && !c->tl) return;
 
   node_prefactors np;
   node_setup(c, i, &np);
@@ -447,6 +467,20 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
         }
       np.num_next = nn;
       np.num_prev = pp;
+    }
+    /* HierarchyUpdater::Get (hierarchy_updater.h:43-49): a node of the
+     * deepest tier (is_timelocal_truncated, hierarchy_integrator.cc:1324-1333)
+     * takes DoTimelocal instead of DoNext.  IndependentBath::DoTimelocal
+     * (hierarchy_updater.cc:171-190): temp = Q_m rho - rho Q_m^+, then
+     * column m += temp[:, m] and row m -= temp[m, :]. */
+    if (c->tl && c->tier[i] == c->trunc - 1) {
+      for (int m = 0; m < N; ++m) {
+        hemm_right(N, 1, r, c->tlq + (size_t)m * E, 0, temp);
+        hemm_left(N, -1, r, c->tlqa + (size_t)m * E, 1, temp);
+        for (int n = 0; n < N; ++n) d[m * N + n] += temp[m * N + n];
+        for (int n = 0; n < N; ++n) d[m + n * N] -= temp[m + n * N];
+      }
+      np.num_next = 0;
     }
     /* IndependentBath::DoNext (:216-233): column m += p rho+[:, m];
      * row m -= p rho+[m, :]. */
@@ -537,6 +571,86 @@ void oracle_initial_state(const oracle_ctx *c, const double *rho0, double *state
 
 /* ------------------------------------------------------------------------ */
 
+/* ConjugateTranspose (complex_matrix.cc:35-44). */
+static void conj_transpose(int N, const cplx *A, cplx *Ah) {
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) Ah[i * N + j] = conj(A[j * N + i]);
+}
+
+/* UpdateTimeLocalTruncation (hierarchy_integrator.cc:1675-1693) for a step
+ * of h: FillPropagator (hierarchy.cc:229-237), U = I - i H h (the Hamiltonian
+ * as stored, without 1/hbar), then UpdateTimeLocalTruncationMatrices
+ * (hierarchy.cc:264-341) for every bath m and term k,
+ *   Q_{m,k} <- d_k U^+ (Q_{m,k} + h c_{m,k} |m><m|) U,
+ * d_0 = exp(-gamma_m h), d_k = exp(-nu k h), and Q_m = sum_k Q_{m,k}
+ * (SumMatrices, complex_matrix.cc:49-57).  Steps below 1e-9 are skipped. */
+static void tl_update(const oracle_ctx *c, double h) {
+  if (!c->tl || h < 1e-9) return;
+  const int N = c->N, E = N * N, K1 = c->K1;
+  cplx *U = (cplx *)malloc(sizeof(cplx) * (size_t)E);
+  cplx *Ua = (cplx *)malloc(sizeof(cplx) * (size_t)E);
+  cplx *tmp = (cplx *)calloc((size_t)E, sizeof(cplx));
+  for (int i = 0; i < E; ++i) U[i] = cx(0, -1) * c->H[i] * h + ((i % (N + 1)) == 0 ? cx(1, 0) : cx(0, 0));
+  conj_transpose(N, U, Ua);
+  const double thermal = c->kb * c->temp;
+  const double nu = 2 * kPi * thermal / c->hbar;
+  for (int m = 0; m < c->nb; ++m) {
+    for (int k = 0; k < K1; ++k) {
+      cplx *Q = c->tlqk + ((size_t)m * K1 + k) * E;
+      const cplx cf = h * c->corr[m * K1 + k];
+      const cplx damp = k == 0 ? cx(exp(-c->gamma[m] * h), 0) : cx(exp(-nu * k * h), 0);
+      Q[m * N + m] += cf;  /* AddIndependentBathOperator at (m, m) */
+      gemm(N, damp, Ua, Q, 0, tmp);
+      gemm(N, 1, tmp, U, 0, Q);
+    }
+    cplx *S = c->tlq + (size_t)m * E;
+    memcpy(S, c->tlqk + (size_t)m * K1 * E, sizeof(cplx) * (size_t)E);
+    for (int k = 1; k < K1; ++k) {
+      const cplx *Q = c->tlqk + ((size_t)m * K1 + k) * E;
+      for (int i = 0; i < E; ++i) S[i] = cx(1, 0) * Q[i] + S[i];
+    }
+    conj_transpose(N, S, c->tlqa + (size_t)m * E);
+  }
+  free(U); free(Ua); free(tmp);
+}
+
+/* StoreTimeLocalTruncationMatrices (:1695-1712). */
+static void tl_store(const oracle_ctx *c) {
+  if (!c->tl) return;
+  const size_t nq = (size_t)c->nb * c->N * c->N;
+  memcpy(c->tlq_st, c->tlq, sizeof(cplx) * nq);
+  memcpy(c->tlqk_st, c->tlqk, sizeof(cplx) * nq * (size_t)c->K1);
+}
+
+/* RestoreTimeLocalTruncationMatrices (:1714-1733). */
+static void tl_restore(const oracle_ctx *c) {
+  if (!c->tl) return;
+  const int N = c->N, E = N * N;
+  const size_t nq = (size_t)c->nb * E;
+  memcpy(c->tlq, c->tlq_st, sizeof(cplx) * nq);
+  memcpy(c->tlqk, c->tlqk_st, sizeof(cplx) * nq * (size_t)c->K1);
+  for (int m = 0; m < c->nb; ++m) conj_transpose(N, c->tlq + (size_t)m * E, c->tlqa + (size_t)m * E);
+}
+
+void oracle_reset_time_local(oracle_ctx *c) {
+  if (!c->tl) return;
+  const size_t nq = (size_t)c->nb * c->N * c->N;
+  memset(c->tlqk, 0, sizeof(cplx) * nq * (size_t)c->K1);
+  memset(c->tlqk_st, 0, sizeof(cplx) * nq * (size_t)c->K1);
+  memset(c->tlq, 0, sizeof(cplx) * nq);
+  memset(c->tlq_st, 0, sizeof(cplx) * nq);
+  memset(c->tlqa, 0, sizeof(cplx) * nq);
+}
+
+void oracle_get_time_local(const oracle_ctx *c, double *q) {
+  const size_t nq = (size_t)c->nb * c->N * c->N;
+  if (!c->tl) {
+    memset(q, 0, sizeof(double) * 2 * nq);
+    return;
+  }
+  memcpy(q, c->tlq, sizeof(cplx) * nq);
+}
+
 void oracle_reset_filter(oracle_ctx *c) {
   if (c->active) memset(c->active, 1, (size_t)c->M);
 }
@@ -584,10 +698,12 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start
     i += 1;
     apply_all(c, y, k0, temp);                                   /* :2709-2711 */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k0[j] * h2; /* :2715-2718 */
+    tl_update(c, dt / 2);                                         /* :2721 */
     apply_all(c, x, k1, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k1[j] * h2; /* :2758-2761 */
     apply_all(c, x, k2, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k2[j] * h1; /* :2777-2780 */
+    tl_update(c, dt / 2);                                         /* :2784 */
     apply_all(c, x, k3, temp);
     for (int64_t j = 0; j < total; ++j)                           /* :2822-2825 */
       y[j] += h6 * (k0[j] + 2.0 * k1[j] + 2.0 * k2[j] + k3[j]);
@@ -636,24 +752,35 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
   const int ncoef = (int)(sizeof(coef) / sizeof(coef[0]));
   const cplx dtc = cx(dt0, 0);
   for (int q = 0; q < ncoef; ++q) *coef[q] *= dtc;
+  /* Stage offsets a1..a5 (:1937, :1947-1951), scaled with the step size. */
+  double a[5] = {2. / 9, 1. / 3, 3. / 4, 1.0, 5. / 6};
+  for (int s = 0; s < 5; ++s) a[s] *= mydt;
   double time_now = start_time;
   int64_t i = -1, accepted = 0;
   while (time_now < end_time) {
     i += 1;
     apply_all(c, y, k[0], temp);
+    /* Time-local matrices follow the stage times (:2028, :2079, :2132,
+     * :2188, :2246-2247). */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b10;
+    tl_update(c, a[0]);
     apply_all(c, x, k[1], temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b20 + k[1][j] * b21;
+    tl_update(c, a[1] - a[0]);
     apply_all(c, x, k[2], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b30 + k[1][j] * b31 + k[2][j] * b32;
+    tl_update(c, a[2] - a[1]);
     apply_all(c, x, k[3], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b40 + k[1][j] * b41 + k[2][j] * b42 + k[3][j] * b43;
+    tl_update(c, a[3] - a[2]);
     apply_all(c, x, k[4], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b50 + k[1][j] * b51 + k[2][j] * b52 + k[3][j] * b53 +
              k[4][j] * b54;
+    tl_restore(c);
+    tl_update(c, a[4]);
     apply_all(c, x, k[5], temp);
     /* Fourth- and fifth-order solutions and the global max-abs difference
      * (:2317-2328, :2339-2351); x holds the fifth-order candidate. */
@@ -669,6 +796,8 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
     if (max_diff < tolerance || mydt * creal(dtdn) < min_dt) {
       memcpy(y, x, sizeof(cplx) * (size_t)total);
       update_filter(c, y);                                        /* :2359-2384 */
+      tl_update(c, mydt - a[4]);                                  /* :2388-2389 */
+      tl_store(c);
       time_now += mydt;
       accepted += 1;
       int update_dt = max_diff < tolerance / 10;
@@ -679,10 +808,13 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
       if (update_dt) {
         mydt *= creal(dtup);
         for (int q = 0; q < ncoef; ++q) *coef[q] *= dtup;
+        for (int s = 0; s < 5; ++s) a[s] *= creal(dtup);       /* :2403-2408 */
       }
     } else {
       mydt *= creal(dtdn);
       for (int q = 0; q < ncoef; ++q) *coef[q] *= dtdn;
+      for (int s = 0; s < 5; ++s) a[s] *= creal(dtdn);         /* :2442-2447 */
+      tl_restore(c);                                              /* :2479 */
     }
   }
   if (accepted_out) *accepted_out = accepted;

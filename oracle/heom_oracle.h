@@ -45,6 +45,7 @@ typedef struct {
   const double *lambda;       /* num_baths */
   const double *coupling;     /* diagonal: num_baths*N; full: num_baths*N*N */
   double filter_tolerance;    /* > 0: adaptive hierarchy filtering (IndependentBath) */
+  int time_local;             /* PhiParameters::use_time_local_truncation (IndependentBath) */
 } oracle_problem;
 
 typedef struct oracle_ctx oracle_ctx;
@@ -76,6 +77,14 @@ void oracle_apply(const oracle_ctx *c, const double *rho, double *drho);
  * them after every step (accepted step) and keep them for the next call.
  * oracle_get_active copies M bytes. */
 void oracle_reset_filter(oracle_ctx *c);
+
+/* Time-local truncation state (the Q_{m,k} matrices of every bath and Matsubara
+ * term, their sums Q_m and the stored copies RKF45 restores on a rejected
+ * step): zero at creation and after oracle_reset_time_local; oracle_rk4 /
+ * oracle_rkf45 advance it and keep it for the next call.  oracle_get_time_local
+ * copies the sums Q_m (2 * num_baths * N * N doubles). */
+void oracle_reset_time_local(oracle_ctx *c);
+void oracle_get_time_local(const oracle_ctx *c, double *q);
 void oracle_get_active(const oracle_ctx *c, unsigned char *flags);
 
 /* Initial hierarchy state: rho(0) scaled into node 0, zeros elsewhere

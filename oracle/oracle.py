@@ -33,6 +33,7 @@ class _Problem(ctypes.Structure):
         ("hamiltonian", POINTER(c_double)), ("gamma", POINTER(c_double)),
         ("lambda_", POINTER(c_double)), ("coupling", POINTER(c_double)),
         ("filter_tolerance", c_double),
+        ("time_local", c_int),
     ]
 
 
@@ -63,6 +64,8 @@ def load():
     lib.oracle_apply.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.oracle_initial_state.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.oracle_reset_filter.argtypes = [c_void_p]
+    lib.oracle_reset_time_local.argtypes = [c_void_p]
+    lib.oracle_get_time_local.argtypes = [c_void_p, c_void_p]
     lib.oracle_get_active.argtypes = [c_void_p, c_void_p]
     lib.oracle_rk4.restype = c_int64
     lib.oracle_rk4.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
@@ -112,6 +115,7 @@ class Oracle:
         self.lib = load()
         n = int(p.num_states)
         self.n = n
+        self.num_baths = int(p.num_bath_couplings)
         self.p = p
         keep = []
 
@@ -142,6 +146,8 @@ class Oracle:
         # only with independent baths.
         ft = float(getattr(p, "filter_tolerance", 0.0) or 0.0)
         pr.filter_tolerance = ft if pr.bath_kind == 0 else 0.0
+        # Time-local truncation, restated for independent baths.
+        pr.time_local = 1 if (getattr(p, "use_time_local_truncation", False) and pr.bath_kind == 0) else 0
         self._keep = keep
         self.ctx = self.lib.oracle_create(ctypes.byref(pr))
         if not self.ctx:
@@ -193,11 +199,25 @@ class Oracle:
         self.lib.oracle_get_active(self.ctx, out.ctypes.data)
         return out.astype(bool)
 
-    def rk4(self, state, dt, t_end, output_min_step=0.0, capacity=0, start_time=0.0, keep_filter=False):
-        """RK4 from `state`; the filter flags start all active (a fresh PHI
-        run) unless keep_filter continues those of the previous call."""
-        if not keep_filter:
+    def reset_time_local(self):
+        """Zeroes the time-local truncation matrices (a fresh PHI run)."""
+        self.lib.oracle_reset_time_local(self.ctx)
+
+    def time_local(self):
+        """Time-local truncation sums Q_m, (num_baths, N, N) complex in PHI's
+        column-major storage (element [m, j, i] = Q_m[i, j])."""
+        nb = self.num_baths
+        out = np.zeros(2 * nb * self.n * self.n)
+        self.lib.oracle_get_time_local(self.ctx, out.ctypes.data)
+        return out.view(np.complex128).reshape(nb, self.n, self.n)
+
+    def rk4(self, state, dt, t_end, output_min_step=0.0, capacity=0, start_time=0.0, continue_run=False):
+        """RK4 from `state`.  The filter flags and the time-local matrices
+        start as a fresh PHI run has them unless continue_run keeps those the
+        previous call left."""
+        if not continue_run:
             self.reset_filter()
+            self.reset_time_local()
         s = np.ascontiguousarray(state, np.float64).copy()
         E2 = 2 * self.n * self.n
         traj = np.zeros(max(capacity, 1) * E2)
@@ -211,10 +231,12 @@ class Oracle:
         rows = [_from_colmajor(traj[r * E2:(r + 1) * E2], self.n) for r in range(k)]
         return s, int(steps), times[:k].copy(), np.array(rows)
 
-    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0, keep_filter=False):
-        """RKF45 from `state`; filter flags as for rk4."""
-        if not keep_filter:
+    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0, continue_run=False):
+        """RKF45 from `state`; run state (flags, time-local matrices) as
+        for rk4."""
+        if not continue_run:
             self.reset_filter()
+            self.reset_time_local()
         s = np.ascontiguousarray(state, np.float64).copy()
         acc = c_int64()
         tf = c_double()
@@ -335,6 +357,8 @@ def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_to
     ft = float(getattr(p, "filter_tolerance", 0.0) or 0.0)
     if ft > 0:
         lines.append(f"FilterTolerance={_fmt(ft)}")
+    if getattr(p, "use_time_local_truncation", False):
+        lines.append("TimeLocal=1")
     return "\n".join(lines) + "\n"
 
 

@@ -51,6 +51,7 @@ class PhiParameters:
     rkf45_minimum_timestep: float = 1e-6
     bicgstab_tolerance: float = 1e-6
     filter_tolerance: float = 0.0
+    use_time_local_truncation: bool = False
 
     @property
     def bath_kind(self) -> int:

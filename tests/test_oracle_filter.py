@@ -109,7 +109,7 @@ def test_flags_reactivate():
     o = O.Oracle(p)
     s, *_ = o.rk4(o.initial_state(), 0.001, 0.001)
     first = o.active()
-    s, *_ = o.rk4(s, 0.001, 0.05, start_time=0.001, keep_filter=True)
+    s, *_ = o.rk4(s, 0.001, 0.05, start_time=0.001, continue_run=True)
     last = o.active()
     assert (~first).sum() > 0
     assert (last & ~first).sum() > 0, "no node came back"
@@ -122,7 +122,7 @@ def test_chunked_rk4_keeps_flags():
     o = O.Oracle(p)
     one, n1, *_ = o.rk4(o.initial_state(), 0.001, 0.05)
     a, na, *_ = o.rk4(o.initial_state(), 0.001, 0.013)
-    b, nb, *_ = o.rk4(a, 0.001, 0.05, start_time=0.013, keep_filter=True)
+    b, nb, *_ = o.rk4(a, 0.001, 0.05, start_time=0.013, continue_run=True)
     assert n1 == na + nb
     assert np.abs(b - one).max() <= 1e-14
 
