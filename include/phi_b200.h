@@ -95,6 +95,15 @@ typedef struct {
                                   Ignored for diagonal and full baths, as
                                   FixIncompatibleCombinations drops it
                                   (phi_parameters.cc:847-851).  0 = off. */
+  int32_t time_local;          /* use_time_local_truncation (TimeLocal): 1 turns
+                                  on time-local truncation -- the deepest tier
+                                  takes -sum_m [V_m, Q_m rho - rho Q_m^+] in
+                                  place of its next terms, with the Q_m
+                                  advanced along the integrator's stage times
+                                  (UpdateTimeLocalTruncation,
+                                  hierarchy_integrator.cc:1675-1733;
+                                  hierarchy.cc:229-341).  Independent baths on
+                                  PHI's identity site map only.  0 = off. */
 } phi_problem_desc;
 
 typedef struct phi_ctx phi_ctx;
@@ -154,6 +163,12 @@ PHI_API int phi_gpu_get_state(const phi_ctx *ctx, double *state);
  * 1 = active (HierarchyNode::is_active).  All 1 after create, set_state,
  * reset and restart reads, and always when filtering is off. */
 PHI_API int phi_gpu_get_active(const phi_ctx *ctx, uint8_t *flags);
+
+/* Time-local truncation sums Q_m of the current state, host buffer of
+ * 2*N*N*N doubles: one complex column-major N x N matrix per bath (time-local
+ * truncation runs on PHI's identity site map, so num_baths = N); all zero
+ * when it is off.  Zero after create, set_state and reset. */
+PHI_API int phi_gpu_get_time_local(const phi_ctx *ctx, double *q);
 
 /* rho_0 (node 0), host buffer of 2*N*N doubles.  Replaces density_matrix()
  * (hierarchy_integrator.cc:177-191), which returns the same storage order. */

@@ -63,6 +63,7 @@ class PhiProblemDesc(ctypes.Structure):
         ("device", c_int32),
         ("max_nodes", c_int64),
         ("filter_tolerance", c_double),
+        ("time_local", c_int32),
     ]
 
 
@@ -113,6 +114,7 @@ SIGNATURES = [
     ("phi_gpu_get_state", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_rho0", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_active", c_int, [c_void_p, c_void_p]),
+    ("phi_gpu_get_time_local", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_apply", c_int, [c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_apply_device", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_rk4", c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_void_p, c_int64,

@@ -57,6 +57,11 @@ struct HeomConsts {
   // neighbours until it rises above it again.
   int filtered;
   double filter_tol;
+  // Time-local truncation (PHI's TimeLocal, independent baths on the
+  // identity site map): nodes of the deepest tier add -[V_m, Q_m X - X Q_m^+]
+  // for every bath m (hierarchy_updater.cc:171-190) instead of next terms.
+  int time_local;
+  const double2 *tl_q;       // nb*N*N: the sums Q_m, column-major per bath
 };
 
 // Device control block of the adaptive integrator; lives in device memory and
@@ -79,6 +84,13 @@ struct Rkf45Ctl {
   int done;           // 1 once time >= end_time or the step limit is hit
   int status;         // 0 ok, 1 step limit
   int nonfinite;      // 1 if a non-finite error estimate was seen
+  // Time-local truncation: the stage offsets a1..a5 (scaled with dt like
+  // coef), and what the last control step did -- 1 accepted (the matrices
+  // then advance by tl_h_accept = dt - a5 of that attempt and are stored),
+  // 2 rejected (restored), 0 nothing (run already done).
+  int tl_pending;
+  double a[5];
+  double tl_h_accept;
 };
 
 // RK4 device bookkeeping (only the rho_0 trajectory needs it).

@@ -29,6 +29,7 @@
 #include "heom_device.cuh"
 #include "heom_kernels.h"
 #include "heom_tile.h"
+#include "heom_tl_term.cuh"
 
 namespace phi {
 namespace {
@@ -71,9 +72,10 @@ __host__ __device__ inline SmemPlan smem_plan(int N, int T, int kind) {
   p.E = N * N;
   p.gcols = kind == kIndependent ? 2 * T * N : 2 * N * N;
   p.per_group = 3 * p.E + p.gcols;
-  // ids[2T], nts[T], then two 8-byte slots at an even int offset (the
-  // node's dephasing rate and, when filtering, its max |y|^2).
-  p.ints_per_group = ((3 * T + 1) & ~1) + 4;
+  // ids[2T], nts[T], then three 8-byte slots at an even int offset (the
+  // node's dephasing rate, its max |y|^2 when filtering, and whether it is
+  // in the deepest tier, for time-local truncation).
+  p.ints_per_group = ((3 * T + 1) & ~1) + 6;
   return p;
 }
 
@@ -118,6 +120,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
   int *nts = ids + 2 * T;
   double *deph_s = reinterpret_cast<double *>(ids + ((3 * T + 1) & ~1));  // 8-byte aligned
   unsigned long long *nmax_s = reinterpret_cast<unsigned long long *>(deph_s + 1);
+  int *tlf_s = reinterpret_cast<int *>(nmax_s + 1);
 
   int ycur = 0;
   if (p.mode == kModeRkf45) {
@@ -162,6 +165,9 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
       for (int t = 0; t < T; ++t) d += nts[t] * __ldg(c.nu + t);
       deph_s[0] = d;
       nmax_s[0] = 0ull;
+      int tier = 0;
+      for (int t = 0; t < T; ++t) tier += nts[t];
+      tlf_s[0] = c.time_local && tier == c.L;
     }
     if (KIND == kIndependent && !c.vacuum) {
       for (int idx = lane; idx < 2 * T * N; idx += GROUP) {
@@ -284,6 +290,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
 
     // 4. upper-triangle pairs
     const double deph = deph_s[0];
+    const bool tl_node = tlf_s[0] != 0;
     const int npairs = N * (N + 1) / 2;
     for (int u = lane; u < npairs; u += GROUP) {
       const int i = __ldg(c.pair_i + u), j = __ldg(c.pair_j + u);
@@ -293,6 +300,7 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
       if (!c.vacuum) {
         const double fac = deph + __ldg(c.mats_elem + i + j * N);
         v = c_axpy(v, xij, -fac);
+        if (KIND == kIndependent && tl_node && i != j) v = c_add(v, tl_pair_term<double2>(Xs, c.tl_q, N, i, j));
         if (KIND == kIndependent) {
           if (i != j) {
             for (int q = __ldg(c.site_ptr + j); q < __ldg(c.site_ptr + j + 1); ++q) {
@@ -459,7 +467,11 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
 // step size the attempt was made with.
 __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  if (ctl->done) return;
+  if (ctl->done) {
+    ctl->tl_pending = 0;
+    return;
+  }
+  ctl->tl_pending = 0;
   const double err = __longlong_as_double((long long)ctl->err_bits);
   ctl->err_bits = 0ull;
   ctl->steps += 1;
@@ -470,6 +482,9 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
     return;
   }
   if (err < ctl->tol || ctl->dt * ctl->dtdn < ctl->min_dt) {
+    // Time-local matrices advance by the rest of this attempt (dt - a5).
+    ctl->tl_h_accept = ctl->dt - ctl->a[4];
+    ctl->tl_pending = 1;
     ctl->ycur ^= 1;
     ctl->time += ctl->dt;
     ctl->accepted += 1;
@@ -482,10 +497,13 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
     if (update) {
       ctl->dt *= ctl->dtup;
       for (int q = 0; q < 24; ++q) ctl->coef[q] *= ctl->dtup;
+      for (int q = 0; q < 5; ++q) ctl->a[q] *= ctl->dtup;
     }
   } else {
     ctl->dt *= ctl->dtdn;
     for (int q = 0; q < 24; ++q) ctl->coef[q] *= ctl->dtdn;
+    for (int q = 0; q < 5; ++q) ctl->a[q] *= ctl->dtdn;
+    ctl->tl_pending = 2;
   }
   if (!(ctl->time < ctl->end_time)) ctl->done = 1;
   if (!ctl->done && ctl->steps >= ctl->max_steps) {

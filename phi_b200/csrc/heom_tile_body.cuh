@@ -52,6 +52,7 @@
 #include "heom_device.cuh"
 #include "heom_kernels.h"
 #include "heom_tile.h"
+#include "heom_tl_term.cuh"
 
 namespace phi {
 namespace tile_detail {
@@ -474,6 +475,28 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       Us[nd * EU + i + j * NP] = v;
       v.y = -v.y;
       Us[nd * EU + j + i * NP] = v;
+    }
+  }
+  // Time-local truncation: the deepest tier's term, a pass of its own so the
+  // pair loop above keeps its registers.  Item `it` maps to the thread that
+  // wrote its two slots in the pair loop, so no barrier is needed before it.
+  if (c.time_local) {
+    for (int it = tid; it < items; it += kTileThreads) {
+      const int nd = it / P, u = it - nd * P;
+      const int i = pi[u], j = pj[u];
+      if (i == j) continue;
+      int tier = 0;  // deepest tier only (is_timelocal_truncated)
+      for (int t = 0; t < T; ++t) tier += nts[nd * T + t];
+      if (tier != c.L) continue;
+      const TX tv = tl_pair_term<TX>(Xs + nd * ES, c.tl_q, N, i, j);
+      TX a = Us[nd * EU + i + j * NP];
+      a.x += tv.x;
+      a.y += tv.y;
+      Us[nd * EU + i + j * NP] = a;
+      TX b = Us[nd * EU + j + i * NP];  // the Hermitian partner takes conj(tv)
+      b.x += tv.x;
+      b.y -= tv.y;
+      Us[nd * EU + j + i * NP] = b;
     }
   }
   ok = p.npre == 0 || mbar_wait_bounded(&bars[1], par1);

@@ -26,7 +26,9 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
     return reject("time-dependent (annealing) Hamiltonians are outside this library's scope");
   if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
     return reject("Hilbert-space truncation is outside this library's scope");
-  if (p.use_time_local_truncation) return reject("time-local truncation is outside this library's scope");
+  if (p.use_time_local_truncation &&
+      (p.is_diagonal_bath_coupling || p.is_full_bath_coupling || p.is_multiple_independent_baths))
+    return reject("time-local truncation is built for independent baths on PHI's identity site map");
   if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
   const bool steady = p.run_method == BICGSTAB || p.run_method == BICGSTABL || p.run_method == BICGSTABU;
   if (p.initial_density_matrix == nullptr && !steady && !p.is_restarted)
@@ -62,6 +64,7 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   d->device = p.device;
   d->max_nodes = 0;
   d->filter_tolerance = p.filter_tolerance;  // already 0 for diagonal / full baths
+  d->time_local = p.use_time_local_truncation ? 1 : 0;  // already 0 for the steady-state methods
   return PHI_OK;
 }
 

@@ -19,6 +19,7 @@
 #include "heom_internal.h"
 #include "heom_kernels.h"
 #include "heom_tile.h"
+#include "heom_timelocal.h"
 #include "phi_context.h"
 
 using phi::DeviceBuffer;
@@ -105,9 +106,13 @@ int setup_constants(phi_ctx *ctx) {
   ctx->corr = corr;
   ctx->delta = delta;
 
-  const bool vacuum = d.truncation_level == 1;
+  // A single tier runs PHI's Vacuum updater (unitary part only) unless
+  // time-local truncation is on, which selects NoHierarchyIndependentBath:
+  // unitary + Matsubara + time-local (hierarchy_integrator.cc:1741-1758).
+  const bool single_tier = d.truncation_level == 1;
+  const bool vacuum = single_tier && !d.time_local;
   const bool normalized = d.normalized != 0;
-  if (!vacuum && d.bath_kind != PHI_BATH_DIAGONAL && normalized) {
+  if (!single_tier && d.bath_kind != PHI_BATH_DIAGONAL && normalized) {
     for (int t = 0; t < T; ++t)
       if (!(abs_corr[t] > 0))
         return fail(ctx, PHI_E_INVALID,
@@ -229,8 +234,10 @@ int setup_constants(phi_ctx *ctx) {
   c.err_flag = cb.err_flag.as<int>();
   // FixIncompatibleCombinations keeps filtering for independent baths only
   // (phi_parameters.cc:847-851); a single tier has no neighbours to filter.
-  c.filtered = (d.bath_kind == PHI_BATH_INDEPENDENT && d.filter_tolerance > 0 && !vacuum) ? 1 : 0;
+  c.filtered = (d.bath_kind == PHI_BATH_INDEPENDENT && d.filter_tolerance > 0 && !single_tier) ? 1 : 0;
   c.filter_tol = c.filtered ? d.filter_tolerance : 0.0;
+  c.time_local = d.time_local ? 1 : 0;
+  c.tl_q = nullptr;  // bound once the matrices are allocated
   return PHI_OK;
 }
 
@@ -281,6 +288,22 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
                 "initial density matrix is not Hermitian (PHI's hierarchy keeps every ADO Hermitian)");
   if (!(d.filter_tolerance >= 0) || !std::isfinite(d.filter_tolerance))
     return fail(nullptr, PHI_E_INVALID, "filter_tolerance must be finite and >= 0");
+  if (d.time_local != 0 && d.time_local != 1)
+    return fail(nullptr, PHI_E_INVALID, "time_local must be 0 or 1");
+  if (d.time_local) {
+    // PHI's diagonal-bath time-local term reads its operator table with the
+    // full-matrix stride (hierarchy_updater.cc:92-104 against the per-state
+    // layout of hierarchy.cc:185-197), and its independent-bath matrices put
+    // c at (b, b) whatever site bath b couples to (hierarchy.cc:298-300);
+    // only the independent identity map has a defined result.
+    bool identity = d.bath_kind == PHI_BATH_INDEPENDENT && d.num_baths == N;
+    if (identity && d.bath_sites)
+      for (int b = 0; b < d.num_baths; ++b) identity = identity && d.bath_sites[b] == b;
+    if (!identity)
+      return fail(nullptr, PHI_E_INVALID,
+                  "time-local truncation is built for independent baths on PHI's identity site map "
+                  "(bath j on |j><j|)");
+  }
 
   std::unique_ptr<phi_ctx> ctx(new phi_ctx());
   ctx->desc = d;
@@ -350,6 +373,15 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
                         cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && ctx->c.time_local) {
+    const size_t nq = (size_t)d.num_baths * N * N * sizeof(double2);
+    if (ctx->tl_qk.alloc(nq * d.num_matsubara_terms) != cudaSuccess ||
+        ctx->tl_qk_st.alloc(nq * d.num_matsubara_terms) != cudaSuccess || ctx->tl_q.alloc(nq) != cudaSuccess ||
+        ctx->tl_q_st.alloc(nq) != cudaSuccess)
+      return fail(nullptr, PHI_E_OOM, "time-local matrix allocation failed");
+    ctx->c.tl_q = ctx->tl_q.as<double2>();
+    e = ctx->reset_time_local();
+  }
   if (e == cudaSuccess && ctx->c.filtered) {
     if (ctx->active[0].alloc((size_t)ctx->hier.M) != cudaSuccess || ctx->active[1].alloc((size_t)ctx->hier.M) != cudaSuccess)
       return fail(nullptr, PHI_E_OOM, "filter flag allocation failed");
@@ -403,6 +435,44 @@ cudaError_t phi_ctx::reset_filter() {
   return cudaMemsetAsync(active[0].ptr, 1, (size_t)hier.M, stream);
 }
 
+cudaError_t phi_ctx::reset_time_local() {
+  if (!c.time_local) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(tl_qk.ptr, 0, tl_qk.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tl_qk_st.ptr, 0, tl_qk_st.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tl_q.ptr, 0, tl_q.bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(tl_q_st.ptr, 0, tl_q_st.bytes, stream);
+  return e;
+}
+
+cudaError_t phi_ctx::enqueue_time_local(int op, int stage, double h, cudaStream_t s) {
+  if (!c.time_local) return cudaSuccess;
+  if (op == phi::kTlAdvance && !(h >= 1e-9)) return cudaSuccess;  // skipped as PHI does
+  phi::TlLaunch L;
+  L.c = c;
+  L.op = op;
+  L.stage = stage;
+  L.h = h;
+  L.ctl = ctl.as<phi::Rkf45Ctl>();
+  L.qk = tl_qk.as<double2>();
+  L.qk_st = tl_qk_st.as<double2>();
+  L.q = tl_q.as<double2>();
+  L.q_st = tl_q_st.as<double2>();
+  return phi::launch_tl(L, s);
+}
+
+extern "C" int phi_gpu_get_time_local(const phi_ctx *cctx, double *q) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !q) return PHI_E_INVALID;
+  const size_t n = (size_t)ctx->desc.num_states * ctx->desc.num_states * ctx->desc.num_states;
+  if (!ctx->c.time_local) {
+    std::memset(q, 0, n * sizeof(double2));
+    return PHI_OK;
+  }
+  PHI_CUDA(ctx, cudaMemcpyAsync(q, ctx->tl_q.ptr, n * sizeof(double2), cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
 void phi_ctx::bind_filter(phi::StageLaunch &L, int par) const {
   if (!c.filtered) return;
   L.act[0] = static_cast<uint8_t *>(active[0].ptr);
@@ -426,6 +496,7 @@ extern "C" int phi_gpu_set_state(phi_ctx *ctx, const double *state) {
   if (!ctx || !state) return PHI_E_INVALID;
   PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, state, ctx->state_bytes(), cudaMemcpyHostToDevice, ctx->stream));
   PHI_CUDA(ctx, ctx->reset_filter());
+  PHI_CUDA(ctx, ctx->reset_time_local());
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PHI_OK;
 }
@@ -519,6 +590,7 @@ extern "C" int phi_gpu_reset(phi_ctx *ctx, double time) {
   PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
                                 cudaMemcpyHostToDevice, ctx->stream));
   PHI_CUDA(ctx, ctx->reset_filter());
+  PHI_CUDA(ctx, ctx->reset_time_local());
   ctx->time = time;
   ctx->rkf45_started = false;
   return PHI_OK;

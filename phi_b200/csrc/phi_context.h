@@ -50,6 +50,9 @@ struct phi_ctx {
   // Filtering (c.filtered): active flags, M bytes each.  Between calls the
   // flags of the current state are in active[0].
   phi::DeviceBuffer active[2];
+  // Time-local truncation (c.time_local): Q_{m,k} and the sums Q_m, with the
+  // copies RKF45 stores and restores (see heom_timelocal.cu).
+  phi::DeviceBuffer tl_qk, tl_qk_st, tl_q, tl_q_st;
   int work_level = 0;          // 1: xa/xb, 2: + acc, 3: + RKF45 buffers
 
   // Captured step graphs.
@@ -95,6 +98,10 @@ struct phi_ctx {
   cudaError_t reset_filter();
   // Points a stage launch at the flag buffers (no-op when filtering is off).
   void bind_filter(phi::StageLaunch &L, int par) const;
+  // Zeroes the time-local truncation matrices (a newly set state).
+  cudaError_t reset_time_local();
+  // Enqueues one update of the time-local matrices (no-op when off).
+  cudaError_t enqueue_time_local(int op, int stage, double h, cudaStream_t s);
 };
 
 namespace phi {

@@ -21,6 +21,7 @@
 #include "../../include/phi_b200.h"
 #include "heom_kernels.h"
 #include "heom_tile.h"
+#include "heom_timelocal.h"
 #include "phi_context.h"
 
 namespace {
@@ -106,6 +107,12 @@ cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, int par, cu
   const void *inv[4] = {L.mixed ? ctx->y32.ptr : (const void *)L.y, ctx->xa.ptr, ctx->xb.ptr, ctx->xa.ptr};
   void *outv[4] = {ctx->xa.ptr, ctx->xb.ptr, ctx->xa.ptr, nullptr};
   for (int st = 0; st < 4; ++st) {
+    // Time-local matrices to t + dt/2 before stage 1 and to t + dt before
+    // stage 3 (hierarchy_integrator.cc:2721, :2784).
+    if (st == 1 || st == 3) {
+      cudaError_t e = ctx->enqueue_time_local(phi::kTlAdvance, 0, dt / 2, s);
+      if (e != cudaSuccess) return e;
+    }
     L.stage = st;
     L.x = in[st];
     L.out = outb[st];
@@ -139,6 +146,12 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
   const double2 *in[6] = {nullptr, xa, xb, xa, xb, xa};
   double2 *outb[6] = {xa, xb, xa, xb, xa, nullptr};
   for (int st = 0; st < 6; ++st) {
+    // Time-local matrices along the stage times (hierarchy_integrator.cc
+    // :2028, :2079, :2132, :2188, :2246-2247), steps read on the device.
+    if (st > 0) {
+      cudaError_t e = ctx->enqueue_time_local(phi::kTlRkf45Stage, st, 0.0, s);
+      if (e != cudaSuccess) return e;
+    }
     L.stage = st;
     L.x = in[st];
     L.out = outb[st];
@@ -147,7 +160,10 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
     cudaError_t e = phi::launch_stage(L, s);
     if (e != cudaSuccess) return e;
   }
-  return phi::launch_rkf45_control(L.ctl, s);
+  cudaError_t e = phi::launch_rkf45_control(L.ctl, s);
+  if (e != cudaSuccess) return e;
+  // Accepted: advance to t + dt and store (:2388-2389); rejected: restore (:2479).
+  return ctx->enqueue_time_local(phi::kTlRkf45Post, 0, 0.0, s);
 }
 
 template <class F>
@@ -280,7 +296,11 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
                             13. / 16.,  4. / 27.,  5. / 144., 1. / 9,     9. / 20,      16. / 45,
                             1. / 12,    47. / 450, 12. / 25,  32. / 225,  1. / 30,      6. / 25};
     for (int q = 0; q < 24; ++q) hc.coef[q] = tab[q] * dt0;
+    // Stage offsets a1..a5 (:1937, :1947-1951).
+    const double offs[5] = {2. / 9, 1. / 3, 3. / 4, 1.0, 5. / 6};
+    for (int s = 0; s < 5; ++s) hc.a[s] = offs[s] * dt0;
   }
+  hc.tl_pending = 0;
   hc.time = ctx->time;
   hc.end_time = t_end;
   hc.tol = tol;

@@ -29,6 +29,7 @@
 
 #include "../../include/phi_b200.h"
 #include "heom_kernels.h"
+#include "heom_timelocal.h"
 #include "phi_context.h"
 
 namespace {
@@ -106,6 +107,12 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
     const double2 *in[4] = {y, xa, xb, xa};
     double2 *nxt[4] = {xa, xb, xa, nullptr};
     for (int st = 0; st < 4 && e == cudaSuccess; ++st) {
+      // Time-local matrices to t + dt/2 and t + dt (no allocation: the
+      // context's own buffers).
+      if (st == 1 || st == 3) {
+        e = ctx->enqueue_time_local(phi::kTlAdvance, 0, dt / 2, static_cast<cudaStream_t>(stream));
+        if (e != cudaSuccess) break;
+      }
       L.stage = st;
       L.x = in[st];
       L.out = nxt[st];

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/phi_b200.h"
+#include "phi_context.h"
 
 namespace {
 
@@ -107,6 +108,10 @@ extern "C" int phi_restart_last_error(char *buf, size_t len) {
 
 extern "C" int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->c.time_local) {
+    ctx->error = "write_restart: a time-local run's restart state includes its Q matrices, which these files do not carry";
+    return fail(PHI_E_INVALID, ctx->error);
+  }
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -120,6 +125,10 @@ extern "C" int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double time
 
 extern "C" int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->c.time_local) {
+    ctx->error = "read_restart: a time-local run's restart state includes its Q matrices, which these files do not carry";
+    return fail(PHI_E_INVALID, ctx->error);
+  }
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -136,6 +145,10 @@ extern "C" int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *time
 
 extern "C" int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->c.time_local) {
+    ctx->error = "save_state: a time-local run's restart state includes its Q matrices, which these files do not carry";
+    return fail(PHI_E_INVALID, ctx->error);
+  }
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -156,6 +169,10 @@ extern "C" int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timeste
 
 extern "C" int phi_gpu_load_state(phi_ctx *ctx, const char *path, double *timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->c.time_local) {
+    ctx->error = "load_state: a time-local run's restart state includes its Q matrices, which these files do not carry";
+    return fail(PHI_E_INVALID, ctx->error);
+  }
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);

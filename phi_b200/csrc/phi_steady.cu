@@ -84,6 +84,12 @@ const char *breakdown_text(int code) {
 int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps, const double *guess,
                 bool guess_rho0, phi_solve_stats *stats) {
   if (!ctx) return PHI_E_INVALID;
+  if (ctx->c.time_local) {
+    // FixIncompatibleCombinations turns time-local truncation off for the
+    // BiCGSTAB methods (phi_parameters.cc:837-838).
+    ctx->error = "steady_state: time-local truncation is a propagation feature (PHI turns it off for steady states)";
+    return PHI_E_INVALID;
+  }
   if (ell < 1 || ell > phi::kMaxEll) {
     ctx->error = "steady_state: ell must be in 1.." + std::to_string(phi::kMaxEll);
     return PHI_E_INVALID;

@@ -135,6 +135,7 @@ def problem_desc(p: PhiParameters, precision: int, device: int, max_nodes: int, 
     d.device = device
     d.max_nodes = max_nodes
     d.filter_tolerance = float(p.filter_tolerance or 0.0)
+    d.time_local = 1 if p.use_time_local_truncation else 0
     return d
 
 
@@ -238,6 +239,15 @@ class Hierarchy:
         out = np.zeros(self.num_nodes, np.uint8)
         self._check(self.lib.phi_gpu_get_active(self.ctx, out.ctypes.data))
         return out.astype(bool)
+
+    def time_local(self) -> np.ndarray:
+        """Time-local truncation sums Q_m, (N, N, N) complex in PHI's
+        column-major storage (element [m, j, i] = Q_m[i, j]; one matrix per
+        bath, num_baths = N on the identity site map); zeros when off."""
+        nb = self.n
+        out = np.zeros(2 * nb * self.n * self.n, np.float64)
+        self._check(self.lib.phi_gpu_get_time_local(self.ctx, out.ctypes.data))
+        return out.view(np.complex128).reshape(nb, self.n, self.n)
 
     def rho0(self) -> np.ndarray:
         out = np.zeros(2 * self.n * self.n, np.float64)

@@ -30,7 +30,14 @@ Outputs (committed; the GPU host has no reference tree):
 
     python tests/golden/make_golden.py /root/reference restart   # restart fixture only
     python tests/golden/make_golden.py /root/reference output    # output-file fixture only
+  ref_timelocal.json    time-local truncation (TimeLocal=1): per case, rho_0
+                        with %.17g, for small hierarchies the whole final
+                        state from the restart file, and for RKF45 the sums
+                        over k of the stored Q_{m,k} the restart file ends
+                        with (RK4 never stores them: PHI writes zeros there)
+
     python tests/golden/make_golden.py /root/reference filter    # filtering fixture only
+    python tests/golden/make_golden.py /root/reference timelocal # time-local fixture only
 """
 from __future__ import annotations
 
@@ -204,6 +211,65 @@ def make_filter_fixture():
         json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
 
 
+# (case id, builder, builder kwargs, method, timestep, t_end, FilterTolerance)
+TIMELOCAL_CASES = [
+    ("rand_n3_k2_t3/rk4", "random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2),
+     "rk4", 0.001, 0.05, 0.0),
+    ("rand_n3_k2_t3/rkf45", "random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2),
+     "rkf45", 0.001, 0.05, 0.0),
+    ("rand_n3_k3_t1/rk4", "random_problem", dict(kind="independent", n=3, matsubara=3, truncation=1, seed=3),
+     "rk4", 0.001, 0.05, 0.0),
+    ("rand_n3_k3_t1/rkf45", "random_problem", dict(kind="independent", n=3, matsubara=3, truncation=1, seed=3),
+     "rkf45", 0.001, 0.05, 0.0),
+    ("rand_n4_k1_t4/rk4", "random_problem", dict(kind="independent", n=4, matsubara=1, truncation=4, seed=1),
+     "rk4", 0.001, 0.05, 0.0),
+    ("rand_n3_k2_t4/rkf45/filter1e-3", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=4, seed=2), "rkf45", 0.001, 0.05, 1e-3),
+    ("frenkel7_L2/rkf45", "config:frenkel7", dict(depth=2), "rkf45", 0.001, 0.05, 0.0),
+]
+
+
+def make_timelocal_fixture():
+    outs = []
+    for cid, builder, kw, method, dt, t_end, ft in TIMELOCAL_CASES:
+        p = build(builder, kw)
+        p.use_time_local_truncation = True
+        p.filter_tolerance = ft
+        if method == "rkf45":
+            p.fix_incompatible_combinations("rkf45")
+        n = p.num_states
+        with tempfile.TemporaryDirectory() as d:
+            prm, out, rst, rho_f = (os.path.join(d, x) for x in ("in.prm", "out.txt", "restart.txt", "rho.txt"))
+            with open(prm, "w") as f:
+                f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_file=out)
+                        + f"RestartFile={rst}\nRestartOutputTimeSecs=1\n")
+            try:
+                subprocess.run([O.REF_DRIVER, "run", prm, method, "1", rho_f], check=True, timeout=120,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            except subprocess.TimeoutExpired:
+                print(f"{cid}: TIMEOUT", flush=True)
+                continue
+            rho = O.parse_rho_file(rho_f, n)
+            numbers = parse_restart_state(open(rst).read(), n)
+        M = O.node_count(p.num_bath_couplings * p.num_matsubara_terms, p.hierarchy_truncation_level)
+        E = n * n
+        state, qk = numbers[:M * E], numbers[M * E:]
+        K1 = p.num_matsubara_terms
+        assert len(qk) == p.num_bath_couplings * K1 * E, (cid, len(qk))
+        case = {"id": cid, "builder": builder, "kwargs": kw, "method": method, "timestep": dt, "t_end": t_end,
+                "filter_tolerance": ft, "num_nodes": M,
+                "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}
+        if M <= 100:
+            case["state_6_digits"] = state
+        if method == "rkf45":
+            q = np.array([complex(a, b) for a, b in qk]).reshape(p.num_bath_couplings, K1, E).sum(axis=1)
+            case["q_sums_6_digits"] = [[float(z.real), float(z.imag)] for z in q.reshape(-1)]
+        outs.append(case)
+        print(f"{cid}: M={M}", flush=True)
+    with open(os.path.join(HERE, "ref_timelocal.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
@@ -217,9 +283,13 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "filter":
         make_filter_fixture()
         return
+    if len(sys.argv) > 2 and sys.argv[2] == "timelocal":
+        make_timelocal_fixture()
+        return
     make_restart_fixture()
     make_output_fixture()
     make_filter_fixture()
+    make_timelocal_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)

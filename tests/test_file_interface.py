@@ -25,8 +25,12 @@ def test_unknown_method_is_rejected(tmp_path):
         Hierarchy.from_file(_write(tmp_path, text), "no_such_method")
 
 
-@pytest.mark.parametrize("line", ["TimeLocal=1"], ids=["time_local"])
-def test_out_of_scope_features_are_rejected(tmp_path, line):
-    text = O.param_file_text(configs.frenkel7(depth=2)) + line + "\n"
+def test_time_local_outside_identity_map_is_rejected(tmp_path):
+    """TimeLocal with correlated (diagonal) bath couplings: PHI's term for
+    them reads its operator table with the wrong stride, so the library
+    refuses the input instead of guessing."""
+    import cases
+    p = cases.random_problem("diagonal", n=3, matsubara=2, truncation=3, seed=1)
+    text = O.param_file_text(p) + "TimeLocal=1\n"
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
         Hierarchy.from_file(_write(tmp_path, text), "rkf45")
