@@ -86,7 +86,7 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
   if (!ctx) return PHI_E_INVALID;
   if (ctx->c.time_local) {
     // FixIncompatibleCombinations turns time-local truncation off for the
-    // BiCGSTAB methods (phi_parameters.cc:837-838).
+    // BiCGSTAB methods (phi_parameters.cc:831-837).
     ctx->error = "steady_state: time-local truncation is a propagation feature (PHI turns it off for steady states)";
     return PHI_E_INVALID;
   }
