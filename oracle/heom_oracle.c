@@ -11,6 +11,7 @@
 #include "heom_oracle.h"
 
 #include <complex.h>
+#include <float.h>
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -44,6 +45,12 @@ struct oracle_ctx {
   int tl;
   cplx *tlqk, *tlqk_st;    /* nb*K1*N*N */
   cplx *tlq, *tlq_st, *tlqa;  /* nb*N*N */
+  /* Annealing Hamiltonian: H and Hadj above follow the fields. */
+  int anneal;
+  cplx *hx, *hz;
+  struct spline { int n, last; double *x, *a, *b, *c, *d; } sx, sz;
+  double old_fx, old_fz;          /* old_*_field_value_th_ */
+  double integration_time, min_field_change;
 };
 
 /* ------------------------------------------------------------------------ */
@@ -163,6 +170,97 @@ int64_t oracle_build_hierarchy(int T, int truncation, int32_t *mi, int64_t capac
 
 static cplx cx(double re, double im) { return CMPLX(re, im); }
 
+/* CubicSpline (cubic_spline.cc:4-120) over n samples on x_i = i / (n - 1).
+ * PHI's construction as written: b_0 = 3 (y_1 - y_0), b_{n-1} =
+ * 3 (y_{n-1} - y_{n-2}), b_i = 3 (y_{i+1} - y_i) otherwise, solved against
+ * the tridiagonal (2, 4, ..., 4, 2 | 1) by L D L^T (dpttrf / dpttrs), then
+ * c_i = 3 (a_{i+1} - a_i) - 2 b_i - b_{i+1}, d_i = 2 (a_i - a_{i+1}) + b_i +
+ * b_{i+1}. */
+static void spline_init(struct spline *s, const double *y, int n) {
+  s->n = n;
+  s->last = 0;
+  s->x = (double *)malloc(sizeof(double) * (size_t)n);
+  s->a = (double *)malloc(sizeof(double) * (size_t)n);
+  s->b = (double *)malloc(sizeof(double) * (size_t)n);
+  s->c = (double *)malloc(sizeof(double) * (size_t)n);
+  s->d = (double *)malloc(sizeof(double) * (size_t)n);
+  const double ds = 1. / (n - 1);
+  for (int i = 0; i < n; ++i) s->x[i] = i * ds;
+  for (int i = 0; i < n; ++i) s->a[i] = y[i];
+  s->b[0] = 3. * (y[1] - y[0]);
+  s->b[n - 1] = 3. * (y[n - 1] - y[n - 2]);
+  for (int i = 1; i < n - 1; ++i) s->b[i] = 3. * (y[i + 1] - y[i]);
+  double *dg = (double *)malloc(sizeof(double) * (size_t)n);
+  double *e = (double *)malloc(sizeof(double) * (size_t)n);
+  dg[0] = dg[n - 1] = 2.;
+  for (int i = 1; i < n - 1; ++i) dg[i] = 4.;
+  for (int i = 0; i < n - 1; ++i) e[i] = 1.;
+  for (int i = 0; i < n - 1; ++i) {  /* factorisation */
+    const double ei = e[i];
+    e[i] = ei / dg[i];
+    dg[i + 1] = dg[i + 1] - e[i] * ei;
+  }
+  double *x = s->b;                   /* forward, diagonal, backward */
+  for (int i = 1; i < n; ++i) x[i] = x[i] - x[i - 1] * e[i - 1];
+  x[n - 1] = x[n - 1] / dg[n - 1];
+  for (int i = n - 2; i >= 0; --i) x[i] = x[i] / dg[i] - x[i + 1] * e[i];
+  free(dg);
+  free(e);
+  for (int i = 0; i < n - 1; ++i) {
+    s->c[i] = 3. * (s->a[i + 1] - s->a[i]) - 2. * s->b[i] - s->b[i + 1];
+    s->d[i] = 2. * (s->a[i] - s->a[i + 1]) + s->b[i] + s->b[i + 1];
+  }
+}
+
+/* CubicSpline::Locate / Get (cubic_spline.cc:33-81): the interval search
+ * starts from the last interval found. */
+static double spline_get(struct spline *s, double x) {
+  if (x > s->x[s->n - 1]) return s->a[s->n - 1];
+  if (x < s->x[0]) return s->a[0];
+  int i;
+  if (x > s->x[s->last] && x < s->x[s->last + 1]) {
+    i = s->last;
+  } else {
+    i = s->last;
+    while (x > s->x[i + 1]) ++i;
+    while (x < s->x[i]) --i;
+    s->last = i;
+  }
+  const double t = (x - s->x[i]) / (s->x[i + 1] - s->x[i]);
+  return s->a[i] + s->b[i] * t + s->c[i] * t * t + s->d[i] * t * t * t;
+}
+
+void oracle_get_hamiltonian(const oracle_ctx *c, double *h) {
+  memcpy(h, c->H, sizeof(cplx) * (size_t)(c->N * c->N));
+}
+
+void oracle_reset_hamiltonian(oracle_ctx *c) {
+  if (!c->anneal) return;
+  const int E = c->N * c->N;
+  for (int k = 0; k < E; ++k) c->H[k] = c->Hadj[k] = 0;
+  c->old_fx = c->old_fz = DBL_MAX;   /* numeric_limits<Float>::max() (:518-523) */
+  c->sx.last = c->sz.last = 0;
+}
+
+/* UpdateTimeDependentHamiltonian (hierarchy_integrator.cc:1618-1673), no
+ * Hilbert-space truncation: H = f_x H_X + f_z H_Z at alpha = t / T, applied
+ * only when either field moved by at least the minimum relative change. */
+static void anneal_update(const oracle_ctx *cc, double time) {
+  oracle_ctx *c = (oracle_ctx *)cc;
+  if (!c->anneal) return;
+  const double alpha = time / c->integration_time;
+  const cplx fx = spline_get(&c->sx, alpha), fz = spline_get(&c->sz, alpha);
+  const double chx = fabs(creal(fx) / c->old_fx - 1.);
+  const double chz = fabs(creal(fz) / c->old_fz - 1.);
+  if (chx < c->min_field_change && chz < c->min_field_change) return;
+  c->old_fx = creal(fx);
+  c->old_fz = creal(fz);
+  const int N = c->N;
+  for (int k = 0; k < N * N; ++k) c->H[k] = fx * c->hx[k] + fz * c->hz[k];
+  for (int r = 0; r < N; ++r)
+    for (int col = 0; col < N; ++col) c->Hadj[r + col * N] = conj(c->H[col + r * N]);
+}
+
 oracle_ctx *oracle_create(const oracle_problem *p) {
   oracle_ctx *c = (oracle_ctx *)calloc(1, sizeof(oracle_ctx));
   if (!c) return NULL;
@@ -231,9 +329,26 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
 
   c->H = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
   c->Hadj = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
-  for (int k = 0; k < N * N; ++k) c->H[k] = cx(p->hamiltonian[2 * k], p->hamiltonian[2 * k + 1]);
-  for (int r = 0; r < N; ++r)  /* ConjugateTranspose (complex_matrix.cc) */
-    for (int col = 0; col < N; ++col) c->Hadj[r + col * N] = conj(c->H[col + r * N]);
+  if (p->h_x) {
+    /* Annealing: the Hamiltonian stays zero until the first update
+     * (hierarchy_integrator.cc:891-944 copies no static H). */
+    c->anneal = 1;
+    c->hx = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
+    c->hz = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
+    for (int k = 0; k < N * N; ++k) {
+      c->hx[k] = cx(p->h_x[2 * k], p->h_x[2 * k + 1]);
+      c->hz[k] = cx(p->h_z[2 * k], p->h_z[2 * k + 1]);
+    }
+    spline_init(&c->sx, p->field_x, p->num_field_x);
+    spline_init(&c->sz, p->field_z, p->num_field_z);
+    c->integration_time = p->integration_time;
+    c->min_field_change = p->min_field_change;
+    oracle_reset_hamiltonian(c);
+  } else {
+    for (int k = 0; k < N * N; ++k) c->H[k] = cx(p->hamiltonian[2 * k], p->hamiltonian[2 * k + 1]);
+    for (int r = 0; r < N; ++r)  /* ConjugateTranspose (complex_matrix.cc) */
+      for (int col = 0; col < N; ++col) c->Hadj[r + col * N] = conj(c->H[col + r * N]);
+  }
 
   /* Correlation-function constants, hierarchy_integrator.cc:427-473. */
   const double hbar = p->hbar;
@@ -319,6 +434,9 @@ void oracle_destroy(oracle_ctx *c) {
   free(c->H); free(c->Hadj); free(c->corr); free(c->abs_corr); free(c->matsubara); free(c->gamma);
   free(c->bath); free(c->same); free(c->nextop); free(c->prevop); free(c->active);
   free(c->tlqk); free(c->tlqk_st); free(c->tlq); free(c->tlq_st); free(c->tlqa);
+  free(c->hx); free(c->hz);
+  free(c->sx.x); free(c->sx.a); free(c->sx.b); free(c->sx.c); free(c->sx.d);
+  free(c->sz.x); free(c->sz.a); free(c->sz.b); free(c->sz.c); free(c->sz.d);
   free(c);
 }
 
@@ -696,14 +814,17 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start
   int64_t i = -1, nout = 0;
   while (time_now < end_time) {
     i += 1;
+    anneal_update(c, time_now);                                   /* :2688 */
     apply_all(c, y, k0, temp);                                   /* :2709-2711 */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k0[j] * h2; /* :2715-2718 */
     tl_update(c, dt / 2);                                         /* :2721 */
+    anneal_update(c, time_now + dt / 2);                          /* :2728 */
     apply_all(c, x, k1, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k1[j] * h2; /* :2758-2761 */
     apply_all(c, x, k2, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k2[j] * h1; /* :2777-2780 */
     tl_update(c, dt / 2);                                         /* :2784 */
+    anneal_update(c, time_now + dt);                              /* :2792 */
     apply_all(c, x, k3, temp);
     for (int64_t j = 0; j < total; ++j)                           /* :2822-2825 */
       y[j] += h6 * (k0[j] + 2.0 * k1[j] + 2.0 * k2[j] + k3[j]);
@@ -759,28 +880,35 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
   int64_t i = -1, accepted = 0;
   while (time_now < end_time) {
     i += 1;
+    anneal_update(c, time_now);                                   /* :1988 */
     apply_all(c, y, k[0], temp);
-    /* Time-local matrices follow the stage times (:2028, :2079, :2132,
-     * :2188, :2246-2247). */
+    /* Time-local matrices and an annealing Hamiltonian follow the stage
+     * times (:1988, :2028-2033, :2079-2084, :2132-2138, :2188-2194,
+     * :2246-2252). */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b10;
     tl_update(c, a[0]);
+    anneal_update(c, time_now + a[0]);
     apply_all(c, x, k[1], temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b20 + k[1][j] * b21;
     tl_update(c, a[1] - a[0]);
+    anneal_update(c, time_now + a[1]);
     apply_all(c, x, k[2], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b30 + k[1][j] * b31 + k[2][j] * b32;
     tl_update(c, a[2] - a[1]);
+    anneal_update(c, time_now + a[2]);
     apply_all(c, x, k[3], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b40 + k[1][j] * b41 + k[2][j] * b42 + k[3][j] * b43;
     tl_update(c, a[3] - a[2]);
+    anneal_update(c, time_now + a[3]);
     apply_all(c, x, k[4], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b50 + k[1][j] * b51 + k[2][j] * b52 + k[3][j] * b53 +
              k[4][j] * b54;
     tl_restore(c);
     tl_update(c, a[4]);
+    anneal_update(c, time_now + a[4]);
     apply_all(c, x, k[5], temp);
     /* Fourth- and fifth-order solutions and the global max-abs difference
      * (:2317-2328, :2339-2351); x holds the fifth-order candidate. */

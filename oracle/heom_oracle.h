@@ -46,6 +46,14 @@ typedef struct {
   const double *coupling;     /* diagonal: num_baths*N; full: num_baths*N*N */
   double filter_tolerance;    /* > 0: adaptive hierarchy filtering (IndependentBath) */
   int time_local;             /* PhiParameters::use_time_local_truncation (IndependentBath) */
+  /* Annealing Hamiltonian (time_indepenent_hamiltonian NULL in PHI):
+   * H(t) = f_x(t/T) H_X + f_z(t/T) H_Z.  hamiltonian is ignored when h_x is
+   * set.  2*N*N complex column-major each; fields sampled on [0, 1]. */
+  const double *h_x, *h_z;
+  const double *field_x, *field_z;
+  int num_field_x, num_field_z;   /* >= 2 each */
+  double integration_time;        /* T (PhiParameters::integration_time) */
+  double min_field_change;        /* PhiParameters::minimum_field_change */
 } oracle_problem;
 
 typedef struct oracle_ctx oracle_ctx;
@@ -84,6 +92,14 @@ void oracle_reset_filter(oracle_ctx *c);
  * oracle_rkf45 advance it and keep it for the next call.  oracle_get_time_local
  * copies the sums Q_m (2 * num_baths * N * N doubles). */
 void oracle_reset_time_local(oracle_ctx *c);
+
+/* Annealing Hamiltonian state (the current H, the last applied field values,
+ * the spline search positions): H zero, fields unset after creation and
+ * oracle_reset_hamiltonian; oracle_rk4 / oracle_rkf45 update H before every
+ * stage (hierarchy_integrator.cc:1988-2252, :2688-2792) and keep the state
+ * for the next call.  oracle_get_hamiltonian copies H (2*N*N doubles). */
+void oracle_reset_hamiltonian(oracle_ctx *c);
+void oracle_get_hamiltonian(const oracle_ctx *c, double *h);
 void oracle_get_time_local(const oracle_ctx *c, double *q);
 void oracle_get_active(const oracle_ctx *c, unsigned char *flags);
 

@@ -34,6 +34,10 @@ class _Problem(ctypes.Structure):
         ("lambda_", POINTER(c_double)), ("coupling", POINTER(c_double)),
         ("filter_tolerance", c_double),
         ("time_local", c_int),
+        ("h_x", POINTER(c_double)), ("h_z", POINTER(c_double)),
+        ("field_x", POINTER(c_double)), ("field_z", POINTER(c_double)),
+        ("num_field_x", c_int), ("num_field_z", c_int),
+        ("integration_time", c_double), ("min_field_change", c_double),
     ]
 
 
@@ -65,6 +69,8 @@ def load():
     lib.oracle_initial_state.argtypes = [c_void_p, c_void_p, c_void_p]
     lib.oracle_reset_filter.argtypes = [c_void_p]
     lib.oracle_reset_time_local.argtypes = [c_void_p]
+    lib.oracle_reset_hamiltonian.argtypes = [c_void_p]
+    lib.oracle_get_hamiltonian.argtypes = [c_void_p, c_void_p]
     lib.oracle_get_time_local.argtypes = [c_void_p, c_void_p]
     lib.oracle_get_active.argtypes = [c_void_p, c_void_p]
     lib.oracle_rk4.restype = c_int64
@@ -134,7 +140,8 @@ class Oracle:
         pr.hbar = float(p.hbar)
         pr.kb = float(p.boltzmann_constant)
         pr.temperature = float(p.temperature)
-        pr.hamiltonian = arr(_colmajor(p.time_indepenent_hamiltonian))
+        H0 = p.time_indepenent_hamiltonian
+        pr.hamiltonian = arr(_colmajor(H0 if H0 is not None else np.zeros((n, n))))
         pr.gamma = arr(p.gamma)
         pr.lambda_ = arr(p.lambda_)
         if pr.bath_kind == 1:
@@ -148,6 +155,16 @@ class Oracle:
         pr.filter_tolerance = ft if pr.bath_kind == 0 else 0.0
         # Time-local truncation, restated for independent baths.
         pr.time_local = 1 if (getattr(p, "use_time_local_truncation", False) and pr.bath_kind == 0) else 0
+        # Annealing Hamiltonian H(t) = f_x(t/T) H_X + f_z(t/T) H_Z.
+        if getattr(p, "transverse_hamiltonian", None) is not None:
+            pr.h_x = arr(_colmajor(np.asarray(p.transverse_hamiltonian, np.complex128)))
+            pr.h_z = arr(_colmajor(np.asarray(p.longitudinal_hamiltonian, np.complex128)))
+            fx = np.asarray(p.transverse_field, np.float64)
+            fz = np.asarray(p.longitudinal_field, np.float64)
+            pr.field_x, pr.field_z = arr(fx), arr(fz)
+            pr.num_field_x, pr.num_field_z = fx.size, fz.size
+            pr.integration_time = float(p.integration_time)
+            pr.min_field_change = float(p.minimum_field_change)
         self._keep = keep
         self.ctx = self.lib.oracle_create(ctypes.byref(pr))
         if not self.ctx:
@@ -199,6 +216,19 @@ class Oracle:
         self.lib.oracle_get_active(self.ctx, out.ctypes.data)
         return out.astype(bool)
 
+    def reset_run_state(self):
+        """Filter flags, time-local matrices and the annealing Hamiltonian
+        as a fresh PHI run has them."""
+        self.reset_filter()
+        self.reset_time_local()
+        self.lib.oracle_reset_hamiltonian(self.ctx)
+
+    def hamiltonian(self):
+        """The current Hamiltonian (N x N complex)."""
+        out = np.zeros(2 * self.n * self.n)
+        self.lib.oracle_get_hamiltonian(self.ctx, out.ctypes.data)
+        return _from_colmajor(out, self.n)
+
     def reset_time_local(self):
         """Zeroes the time-local truncation matrices (a fresh PHI run)."""
         self.lib.oracle_reset_time_local(self.ctx)
@@ -216,8 +246,7 @@ class Oracle:
         start as a fresh PHI run has them unless continue_run keeps those the
         previous call left."""
         if not continue_run:
-            self.reset_filter()
-            self.reset_time_local()
+            self.reset_run_state()
         s = np.ascontiguousarray(state, np.float64).copy()
         E2 = 2 * self.n * self.n
         traj = np.zeros(max(capacity, 1) * E2)
@@ -235,8 +264,7 @@ class Oracle:
         """RKF45 from `state`; run state (flags, time-local matrices) as
         for rk4."""
         if not continue_run:
-            self.reset_filter()
-            self.reset_time_local()
+            self.reset_run_state()
         s = np.ascontiguousarray(state, np.float64).copy()
         acc = c_int64()
         tf = c_double()
@@ -325,9 +353,22 @@ def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_to
     n = int(p.num_states)
     lines = [f"OutputFile={output_file}", "verbose=-2",
              f"hbar={_fmt(p.hbar)}", f"kB={_fmt(p.boltzmann_constant)}",
-             f"NumStates={n}", "Hamiltonian:"]
-    H = np.asarray(p.time_indepenent_hamiltonian, np.complex128)
-    lines += [_row(H[r]) for r in range(n)]
+             f"NumStates={n}"]
+    if getattr(p, "transverse_hamiltonian", None) is not None:
+        # Annealing Hamiltonian (phi_parameters.cc:363-441).
+        for key, M, fkey, f in (("TransverseHamiltonian", p.transverse_hamiltonian, "TransverseField",
+                                 p.transverse_field),
+                                ("LongitudinalHamiltonian", p.longitudinal_hamiltonian, "LongitudinalField",
+                                 p.longitudinal_field)):
+            M = np.asarray(M, np.complex128)
+            lines.append(key + ":")
+            lines += [_row(M[r]) for r in range(n)]
+            lines.append(f"{fkey}=" + ",".join(_fmt(x) for x in np.asarray(f, np.float64)))
+        lines.append(f"MinimumFieldChange={_fmt(p.minimum_field_change)}")
+    else:
+        lines.append("Hamiltonian:")
+        H = np.asarray(p.time_indepenent_hamiltonian, np.complex128)
+        lines += [_row(H[r]) for r in range(n)]
     lines.append(f"NumCouplingTerms={int(p.num_bath_couplings)}")
     kind = bath_kind(p)
     if kind == 1:

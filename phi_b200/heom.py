@@ -52,6 +52,14 @@ class PhiParameters:
     bicgstab_tolerance: float = 1e-6
     filter_tolerance: float = 0.0
     use_time_local_truncation: bool = False
+    # Annealing Hamiltonian (time_indepenent_hamiltonian None):
+    # H(t) = f_x(t/T) H_X + f_z(t/T) H_Z, f_x / f_z cubic splines through the
+    # field samples on [0, 1], T = integration_time.
+    transverse_hamiltonian: Optional[np.ndarray] = None    # H_X
+    longitudinal_hamiltonian: Optional[np.ndarray] = None  # H_Z
+    transverse_field: Optional[np.ndarray] = None
+    longitudinal_field: Optional[np.ndarray] = None
+    minimum_field_change: float = 0.01
 
     @property
     def bath_kind(self) -> int:
