@@ -6,9 +6,8 @@
 // ReadInputFile / FixIncompatibleCombinations, phi_parameters.cc:93-888):
 // `key=value` scalars, `Key:` matrix blocks read row by row into column-major
 // storage, MatsubaraTerms stored as K+1, HierarchyTruncation counting tier 0.
-// Inputs outside this library's scope (annealing Hamiltonians, Hilbert-space
-// truncation, time-local closure, filtering, restart input, spectra) are read
-// and then rejected by HierarchyIntegrator with a message.
+// Inputs outside this library's scope (Hilbert-space truncation, spectra)
+// are read and then rejected by HierarchyIntegrator with a message.
 #ifndef PHI_B200_PHI_PARAMETERS_H_
 #define PHI_B200_PHI_PARAMETERS_H_
 
@@ -58,6 +57,13 @@ struct PHI_API PhiParameters {
   Complex *time_indepenent_hamiltonian;
   Complex *final_annealing_hamiltonian;
   Complex *initial_annealing_hamiltonian;
+  // Annealing fields (TransverseField / LongitudinalField, sampled on
+  // [0, 1] of the run) and MinimumFieldChange (phi_parameters.h:48-55).
+  Float *initial_hamiltonian_field;
+  int initial_hamiltonian_field_size;
+  Float *final_hamiltonian_field;
+  int final_hamiltonian_field_size;
+  Float minimum_field_change;
 
   Float temperature;
 

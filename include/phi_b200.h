@@ -104,6 +104,22 @@ typedef struct {
                                   hierarchy_integrator.cc:1675-1733;
                                   hierarchy.cc:229-341).  Independent baths on
                                   PHI's identity site map only.  0 = off. */
+  /* Annealing Hamiltonian (PHI's time_indepenent_hamiltonian == NULL case,
+   * UpdateTimeDependentHamiltonian, hierarchy_integrator.cc:1618-1673, no
+   * Hilbert-space truncation): when annealing_h_x is non-NULL, hamiltonian
+   * is ignored and before every RK4 / RKF45 stage at time t
+   *   H = f_x(t / T) H_X + f_z(t / T) H_Z,
+   * f_x / f_z PHI's cubic splines (cubic_spline.cc) through the samples on
+   * [0, 1], applied only when either field moved by minimum_field_change
+   * relative to the last applied value.  H is zero until the first stage. */
+  const double *annealing_h_x;       /* H_X (TransverseHamiltonian): 2*N*N */
+  const double *annealing_h_z;       /* H_Z (LongitudinalHamiltonian): 2*N*N */
+  const double *transverse_field;    /* TransverseField samples */
+  int32_t transverse_field_size;     /* >= 2 */
+  const double *longitudinal_field;  /* LongitudinalField samples */
+  int32_t longitudinal_field_size;   /* >= 2 */
+  double integration_time;           /* T (Time); > 0 */
+  double minimum_field_change;       /* MinimumFieldChange (PHI's default 0.01) */
 } phi_problem_desc;
 
 typedef struct phi_ctx phi_ctx;
@@ -169,6 +185,11 @@ PHI_API int phi_gpu_get_active(const phi_ctx *ctx, uint8_t *flags);
  * truncation runs on PHI's identity site map, so num_baths = N); all zero
  * when it is off.  Zero after create, set_state and reset. */
 PHI_API int phi_gpu_get_time_local(const phi_ctx *ctx, double *q);
+
+/* The Hamiltonian the next stage starts from, host buffer of 2*N*N doubles
+ * (complex column-major): the static one, or an annealing Hamiltonian as
+ * last updated (zero before the first stage, and after set_state / reset). */
+PHI_API int phi_gpu_get_hamiltonian(const phi_ctx *ctx, double *h);
 
 /* rho_0 (node 0), host buffer of 2*N*N doubles.  Replaces density_matrix()
  * (hierarchy_integrator.cc:177-191), which returns the same storage order. */

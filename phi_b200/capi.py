@@ -64,6 +64,14 @@ class PhiProblemDesc(ctypes.Structure):
         ("max_nodes", c_int64),
         ("filter_tolerance", c_double),
         ("time_local", c_int32),
+        ("annealing_h_x", POINTER(c_double)),
+        ("annealing_h_z", POINTER(c_double)),
+        ("transverse_field", POINTER(c_double)),
+        ("transverse_field_size", c_int32),
+        ("longitudinal_field", POINTER(c_double)),
+        ("longitudinal_field_size", c_int32),
+        ("integration_time", c_double),
+        ("minimum_field_change", c_double),
     ]
 
 
@@ -115,6 +123,7 @@ SIGNATURES = [
     ("phi_gpu_get_rho0", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_active", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_time_local", c_int, [c_void_p, c_void_p]),
+    ("phi_gpu_get_hamiltonian", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_apply", c_int, [c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_apply_device", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_rk4", c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_void_p, c_int64,

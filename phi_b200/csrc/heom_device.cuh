@@ -99,6 +99,7 @@ struct Rk4Ctl {
   long long out_factor;  // ceil(output_min_step / dt)
   long long capacity;    // trajectory rows available
   long long nout;        // trajectory rows written
+  double time;           // annealing Hamiltonian: time_now of the step in flight
 };
 
 }  // namespace phi

@@ -22,8 +22,11 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
     return PHI_E_INVALID;
   };
   if (!p.are_parameters_valid || p.run_method == BROKENINPUT) return reject("parameter error");
-  if (p.time_indepenent_hamiltonian == nullptr)
-    return reject("time-dependent (annealing) Hamiltonians are outside this library's scope");
+  const bool annealing = p.time_indepenent_hamiltonian == nullptr;
+  if (annealing && (p.initial_annealing_hamiltonian == nullptr || p.final_annealing_hamiltonian == nullptr ||
+                    p.initial_hamiltonian_field_size < 2 || p.final_hamiltonian_field_size < 2))
+    return reject("an annealing Hamiltonian needs TransverseHamiltonian, LongitudinalHamiltonian and both "
+                  "field arrays (2 samples or more)");
   if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
     return reject("Hilbert-space truncation is outside this library's scope");
   if (p.use_time_local_truncation &&
@@ -65,6 +68,17 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   d->max_nodes = 0;
   d->filter_tolerance = p.filter_tolerance;  // already 0 for diagonal / full baths
   d->time_local = p.use_time_local_truncation ? 1 : 0;  // already 0 for the steady-state methods
+  if (annealing) {
+    d->hamiltonian = nullptr;
+    d->annealing_h_x = reinterpret_cast<const double *>(p.initial_annealing_hamiltonian);
+    d->annealing_h_z = reinterpret_cast<const double *>(p.final_annealing_hamiltonian);
+    d->transverse_field = p.initial_hamiltonian_field;
+    d->transverse_field_size = p.initial_hamiltonian_field_size;
+    d->longitudinal_field = p.final_hamiltonian_field;
+    d->longitudinal_field_size = p.final_hamiltonian_field_size;
+    d->integration_time = p.integration_time;
+    d->minimum_field_change = p.minimum_field_change;
+  }
   return PHI_OK;
 }
 

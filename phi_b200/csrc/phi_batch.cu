@@ -179,6 +179,11 @@ extern "C" int phi_gpu_batch_create(const phi_problem_desc *descs, int32_t count
       g_batch_create_error = "instance " + std::to_string(i) + ": every instance needs the same precision and device";
       return PHI_E_INVALID;
     }
+    if (descs[i].annealing_h_x) {
+      g_batch_create_error = "instance " + std::to_string(i) +
+                             ": annealing Hamiltonians run on single hierarchies (phi_gpu_rk4 / phi_gpu_rkf45)";
+      return PHI_E_INVALID;
+    }
     if (descs[i].time_local) {
       g_batch_create_error = "instance " + std::to_string(i) +
                              ": time-local truncation runs on single hierarchies (phi_gpu_rk4 / phi_gpu_rkf45)";

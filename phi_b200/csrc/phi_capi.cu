@@ -20,6 +20,8 @@
 #include "heom_kernels.h"
 #include "heom_tile.h"
 #include "heom_timelocal.h"
+#include "heom_anneal.h"
+#include <cfloat>
 #include "phi_context.h"
 
 using phi::DeviceBuffer;
@@ -264,14 +266,32 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
     return fail(nullptr, PHI_E_INVALID, "unknown bath_kind");
   if (d.precision != PHI_PREC_FP64 && d.precision != PHI_PREC_MIXED)
     return fail(nullptr, PHI_E_INVALID, "unknown precision");
-  if (!d.hamiltonian || !d.initial_density_matrix || !d.gamma || !d.lambda)
+  const bool annealing = d.annealing_h_x != nullptr;
+  if ((!d.hamiltonian && !annealing) || !d.initial_density_matrix || !d.gamma || !d.lambda)
     return fail(nullptr, PHI_E_INVALID, "hamiltonian, initial_density_matrix, gamma and lambda are required");
+  if (annealing) {
+    if (!d.annealing_h_z || !d.transverse_field || !d.longitudinal_field)
+      return fail(nullptr, PHI_E_INVALID, "an annealing Hamiltonian needs H_X, H_Z and both field arrays");
+    if (d.transverse_field_size < 2 || d.longitudinal_field_size < 2)
+      return fail(nullptr, PHI_E_INVALID, "annealing fields need at least 2 samples each");
+    if (!(d.integration_time > 0) || !std::isfinite(d.integration_time) || !(d.minimum_field_change >= 0) ||
+        !std::isfinite(d.minimum_field_change))
+      return fail(nullptr, PHI_E_INVALID, "annealing needs integration_time > 0 and minimum_field_change >= 0");
+    for (int k = 0; k < 2 * N * N; ++k)
+      if (!std::isfinite(d.annealing_h_x[k]) || !std::isfinite(d.annealing_h_z[k]))
+        return fail(nullptr, PHI_E_INVALID, "non-finite value in H_X or H_Z");
+    for (int k = 0; k < d.transverse_field_size; ++k)
+      if (!std::isfinite(d.transverse_field[k])) return fail(nullptr, PHI_E_INVALID, "non-finite transverse field");
+    for (int k = 0; k < d.longitudinal_field_size; ++k)
+      if (!std::isfinite(d.longitudinal_field[k]))
+        return fail(nullptr, PHI_E_INVALID, "non-finite longitudinal field");
+  }
   if (!(d.hbar > 0) || !(d.boltzmann_constant > 0) || !(d.temperature > 0))
     return fail(nullptr, PHI_E_INVALID, "hbar, boltzmann_constant and temperature must be positive");
   if (d.bath_kind != PHI_BATH_INDEPENDENT && !d.coupling)
     return fail(nullptr, PHI_E_INVALID, "diagonal and full baths need coupling operators");
   for (int k = 0; k < 2 * N * N; ++k)
-    if (!std::isfinite(d.hamiltonian[k]) || !std::isfinite(d.initial_density_matrix[k]))
+    if ((!annealing && !std::isfinite(d.hamiltonian[k])) || !std::isfinite(d.initial_density_matrix[k]))
       return fail(nullptr, PHI_E_INVALID, "non-finite value in the Hamiltonian or initial density matrix");
   if (d.truncation_level > 1 && (d.normalized || d.bath_kind == PHI_BATH_DIAGONAL)) {
     // The normalised prefactors divide by sqrt(n |c_t|) (hierarchy_integrator.cc
@@ -307,7 +327,12 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
 
   std::unique_ptr<phi_ctx> ctx(new phi_ctx());
   ctx->desc = d;
-  ctx->hamiltonian.assign(d.hamiltonian, d.hamiltonian + 2 * N * N);
+  // An annealing Hamiltonian starts at zero (PHI copies no static H).
+  if (annealing)
+    ctx->hamiltonian.assign((size_t)2 * N * N, 0.0);
+  else
+    ctx->hamiltonian.assign(d.hamiltonian, d.hamiltonian + 2 * N * N);
+  ctx->annealing = annealing;
   ctx->rho_init.assign(d.initial_density_matrix, d.initial_density_matrix + 2 * N * N);
   ctx->gamma.assign(d.gamma, d.gamma + d.num_baths);
   ctx->lambda.assign(d.lambda, d.lambda + d.num_baths);
@@ -340,6 +365,8 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   ctx->desc.initial_density_matrix = nullptr;
   ctx->desc.gamma = ctx->desc.lambda = ctx->desc.coupling = nullptr;
   ctx->desc.bath_sites = nullptr;
+  ctx->desc.annealing_h_x = ctx->desc.annealing_h_z = nullptr;
+  ctx->desc.transverse_field = ctx->desc.longitudinal_field = nullptr;
 
   cudaError_t e = cudaSetDevice(d.device);
   if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
@@ -373,6 +400,30 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(ctx->y.ptr, ctx->rho_init.data(), (size_t)N * N * sizeof(double2),
                         cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && annealing) {
+    const size_t hb = (size_t)N * N * sizeof(double2);
+    const int nx = d.transverse_field_size, nz = d.longitudinal_field_size;
+    std::vector<double> coef((size_t)5 * (nx + nz));
+    phi::anneal_spline_host(d.transverse_field, nx, coef.data());
+    phi::anneal_spline_host(d.longitudinal_field, nz, coef.data() + 5 * nx);
+    if (ctx->an_hx.alloc(hb) != cudaSuccess || ctx->an_hz.alloc(hb) != cudaSuccess ||
+        ctx->an_spline.alloc(coef.size() * sizeof(double)) != cudaSuccess ||
+        ctx->an_state.alloc(sizeof(phi::AnnealState)) != cudaSuccess)
+      return fail(nullptr, PHI_E_OOM, "annealing buffer allocation failed");
+    ctx->an_nx = nx;
+    ctx->an_nz = nz;
+    e = cudaMemcpyAsync(ctx->an_hx.ptr, d.annealing_h_x, hb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->an_hz.ptr, d.annealing_h_z, hb, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ctx->an_spline.ptr, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // coef is a local buffer
+    // The real-H fast path of the tiled kernel holds when H_X and H_Z are real.
+    ctx->c.h_real = 1;
+    for (int k = 0; k < N * N; ++k)
+      if (d.annealing_h_x[2 * k + 1] != 0.0 || d.annealing_h_z[2 * k + 1] != 0.0) ctx->c.h_real = 0;
+    if (e == cudaSuccess) e = ctx->reset_annealing();
+  }
   if (e == cudaSuccess && ctx->c.time_local) {
     const size_t nq = (size_t)d.num_baths * N * N * sizeof(double2);
     if (ctx->tl_qk.alloc(nq * d.num_matsubara_terms) != cudaSuccess ||
@@ -460,6 +511,46 @@ cudaError_t phi_ctx::enqueue_time_local(int op, int stage, double h, cudaStream_
   return phi::launch_tl(L, s);
 }
 
+cudaError_t phi_ctx::reset_annealing() {
+  if (!annealing) return cudaSuccess;
+  const phi::AnnealState st{DBL_MAX, DBL_MAX, 0, 0};  // numeric_limits<Float>::max() (:518-523)
+  cudaError_t e = cudaMemcpyAsync(an_state.ptr, &st, sizeof(st), cudaMemcpyHostToDevice, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(cbuf.H.ptr, 0, cbuf.H.bytes, stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // st is a local
+  return e;
+}
+
+cudaError_t phi_ctx::enqueue_anneal(int op, int which, double dt, cudaStream_t s) {
+  if (!annealing) return cudaSuccess;
+  phi::AnnealLaunch L;
+  L.op = op;
+  L.which = which;
+  L.dt = dt;
+  L.rk4 = ctl.as<phi::Rk4Ctl>();
+  L.ctl = ctl.as<phi::Rkf45Ctl>();
+  const double *sp = an_spline.as<double>();
+  L.sx = phi::AnnealSpline{sp, sp + an_nx, sp + 2 * an_nx, sp + 3 * an_nx, sp + 4 * an_nx, an_nx};
+  const double *sz = sp + 5 * an_nx;
+  L.sz = phi::AnnealSpline{sz, sz + an_nz, sz + 2 * an_nz, sz + 3 * an_nz, sz + 4 * an_nz, an_nz};
+  L.st = an_state.as<phi::AnnealState>();
+  L.hx = an_hx.as<double2>();
+  L.hz = an_hz.as<double2>();
+  L.H = cbuf.H.as<double2>();
+  L.E = desc.num_states * desc.num_states;
+  L.integration_time = desc.integration_time;
+  L.min_field_change = desc.minimum_field_change;
+  return phi::launch_anneal(L, s);
+}
+
+extern "C" int phi_gpu_get_hamiltonian(const phi_ctx *cctx, double *h) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !h) return PHI_E_INVALID;
+  PHI_CUDA(ctx, cudaMemcpyAsync(h, ctx->cbuf.H.ptr, (size_t)ctx->desc.num_states * ctx->desc.num_states * sizeof(double2),
+                                cudaMemcpyDeviceToHost, ctx->stream));
+  PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
 extern "C" int phi_gpu_get_time_local(const phi_ctx *cctx, double *q) {
   phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
   if (!ctx || !q) return PHI_E_INVALID;
@@ -497,6 +588,7 @@ extern "C" int phi_gpu_set_state(phi_ctx *ctx, const double *state) {
   PHI_CUDA(ctx, cudaMemcpyAsync(ctx->y.ptr, state, ctx->state_bytes(), cudaMemcpyHostToDevice, ctx->stream));
   PHI_CUDA(ctx, ctx->reset_filter());
   PHI_CUDA(ctx, ctx->reset_time_local());
+  PHI_CUDA(ctx, ctx->reset_annealing());
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   return PHI_OK;
 }
@@ -591,6 +683,7 @@ extern "C" int phi_gpu_reset(phi_ctx *ctx, double time) {
                                 cudaMemcpyHostToDevice, ctx->stream));
   PHI_CUDA(ctx, ctx->reset_filter());
   PHI_CUDA(ctx, ctx->reset_time_local());
+  PHI_CUDA(ctx, ctx->reset_annealing());
   ctx->time = time;
   ctx->rkf45_started = false;
   return PHI_OK;

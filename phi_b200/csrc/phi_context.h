@@ -53,6 +53,12 @@ struct phi_ctx {
   // Time-local truncation (c.time_local): Q_{m,k} and the sums Q_m, with the
   // copies RKF45 stores and restores (see heom_timelocal.cu).
   phi::DeviceBuffer tl_qk, tl_qk_st, tl_q, tl_q_st;
+  // Annealing Hamiltonian (desc.annealing_h_x set): H_X, H_Z, the two
+  // splines' coefficients and the update state (see heom_anneal.cu); the
+  // stage kernels read H from cbuf.H.
+  bool annealing = false;
+  phi::DeviceBuffer an_hx, an_hz, an_spline, an_state;
+  int an_nx = 0, an_nz = 0;
   int work_level = 0;          // 1: xa/xb, 2: + acc, 3: + RKF45 buffers
 
   // Captured step graphs.
@@ -102,6 +108,10 @@ struct phi_ctx {
   cudaError_t reset_time_local();
   // Enqueues one update of the time-local matrices (no-op when off).
   cudaError_t enqueue_time_local(int op, int stage, double h, cudaStream_t s);
+  // Annealing: H zero and the update state of a fresh run.
+  cudaError_t reset_annealing();
+  // Enqueues one annealing update (no-op without annealing).
+  cudaError_t enqueue_anneal(int op, int which, double dt, cudaStream_t s);
 };
 
 namespace phi {

@@ -22,6 +22,7 @@
 #include "heom_kernels.h"
 #include "heom_tile.h"
 #include "heom_timelocal.h"
+#include "heom_anneal.h"
 #include "phi_context.h"
 
 namespace {
@@ -113,6 +114,11 @@ cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, int par, cu
       cudaError_t e = ctx->enqueue_time_local(phi::kTlAdvance, 0, dt / 2, s);
       if (e != cudaSuccess) return e;
     }
+    // Annealing Hamiltonian at t, t + dt/2 and t + dt (:2688, :2728, :2792).
+    if (st != 2) {
+      cudaError_t e = ctx->enqueue_anneal(phi::kAnnealRk4, st == 0 ? 0 : (st == 1 ? 1 : 2), dt, s);
+      if (e != cudaSuccess) return e;
+    }
     L.stage = st;
     L.x = in[st];
     L.out = outb[st];
@@ -150,6 +156,11 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
     // :2028, :2079, :2132, :2188, :2246-2247), steps read on the device.
     if (st > 0) {
       cudaError_t e = ctx->enqueue_time_local(phi::kTlRkf45Stage, st, 0.0, s);
+      if (e != cudaSuccess) return e;
+    }
+    // Annealing Hamiltonian at t + a_s (:1988, :2033, :2084, :2138, :2194, :2252).
+    {
+      cudaError_t e = ctx->enqueue_anneal(phi::kAnnealRkf45, st, 0.0, s);
       if (e != cudaSuccess) return e;
     }
     L.stage = st;
@@ -224,6 +235,7 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
     PHI_CK(phi::launch_to_c64(ctx->y.as<double2>(), ctx->y32.as<float2>(), ctx->hier.M,
                               ctx->desc.num_states * ctx->desc.num_states, ctx->work_stride(), ctx->stream));
   phi::Rk4Ctl hc{};
+  hc.time = ctx->time;
   hc.step = 0;
   hc.out_factor = out_factor;
   hc.capacity = rows;

@@ -76,6 +76,10 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
     ctx->error = "rk4_step_noalloc: complex128 (PHI_PREC_FP64) contexts only";
     return PHI_E_INVALID;
   }
+  if (ctx->annealing) {
+    ctx->error = "rk4_step_noalloc: an annealing Hamiltonian follows the step time kept by phi_gpu_rk4";
+    return PHI_E_INVALID;
+  }
   const size_t bytes = ctx->state_bytes();
   if (bytes > kNoAllocMaxStateBytes) {
     ctx->error = "rk4_step_noalloc: hierarchy state of " + std::to_string(bytes) +

@@ -13,6 +13,7 @@
 // ParameterInput::ReadValue (parameter_input.cc:10-44).
 #include "../../include/phi/phi_parameters.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -162,6 +163,11 @@ PhiParameters::PhiParameters() {
   time_indepenent_hamiltonian = nullptr;
   final_annealing_hamiltonian = nullptr;
   initial_annealing_hamiltonian = nullptr;
+  initial_hamiltonian_field = nullptr;
+  initial_hamiltonian_field_size = 0;
+  final_hamiltonian_field = nullptr;
+  final_hamiltonian_field_size = 0;
+  minimum_field_change = 0.01;
   gamma = lambda = bath_coupling_op = nullptr;
   multiple_independent_bath_indices = nullptr;
   initial_density_matrix = nullptr;
@@ -172,6 +178,8 @@ PhiParameters::~PhiParameters() {
   delete[] time_indepenent_hamiltonian;
   delete[] final_annealing_hamiltonian;
   delete[] initial_annealing_hamiltonian;
+  delete[] initial_hamiltonian_field;
+  delete[] final_hamiltonian_field;
   delete[] gamma;
   delete[] lambda;
   delete[] bath_coupling_op;
@@ -393,6 +401,19 @@ void PhiParameters::ReadInputFile(std::string parameter_file) {
       if (!parse_real_row(val, num_bath_couplings, &v)) { bad("ERROR: incorrect " + key + " input format.\n"); break; }
       *dst = zeros<Float>(num_bath_couplings);
       for (int i = 0; i < num_bath_couplings; ++i) (*dst)[i] = v[i];
+    } else if (key == "TransverseField" || key == "LongitudinalField") {
+      // Comma-separated samples (phi_parameters.cc:385-433).
+      const int count = (int)std::count(val.begin(), val.end(), ',') + 1;
+      std::vector<double> v;
+      if (!parse_real_row(val, count, &v)) { bad("ERROR: incorrect " + key + " input format.\n"); break; }
+      Float **dst = key == "TransverseField" ? &initial_hamiltonian_field : &final_hamiltonian_field;
+      int *size = key == "TransverseField" ? &initial_hamiltonian_field_size : &final_hamiltonian_field_size;
+      delete[] *dst;
+      *dst = zeros<Float>(count);
+      for (int i = 0; i < count; ++i) (*dst)[i] = v[i];
+      *size = count;
+    } else if (key == "MinimumFieldChange") {
+      if (!parse_double(val, key, &minimum_field_change, kNonNegative)) { are_parameters_valid = false; break; }
     } else if (key == "kappa") {
       has_kappa = true;
     } else if (key == "T" || key == "Temperature") {

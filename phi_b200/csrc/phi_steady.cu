@@ -84,6 +84,10 @@ const char *breakdown_text(int code) {
 int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps, const double *guess,
                 bool guess_rho0, phi_solve_stats *stats) {
   if (!ctx) return PHI_E_INVALID;
+  if (ctx->annealing) {
+    ctx->error = "steady_state: an annealing Hamiltonian has no steady state (it changes with time)";
+    return PHI_E_INVALID;
+  }
   if (ctx->c.time_local) {
     // FixIncompatibleCombinations turns time-local truncation off for the
     // BiCGSTAB methods (phi_parameters.cc:831-837).

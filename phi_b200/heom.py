@@ -126,7 +126,17 @@ def problem_desc(p: PhiParameters, precision: int, device: int, max_nodes: int, 
         keep_list.append(a)
         return a
 
-    d.hamiltonian = _dptr(keep(col_major(p.time_indepenent_hamiltonian)))
+    if p.transverse_hamiltonian is not None:
+        # Annealing: H(t) = f_x(t/T) H_X + f_z(t/T) H_Z.
+        d.annealing_h_x = _dptr(keep(col_major(p.transverse_hamiltonian)))
+        d.annealing_h_z = _dptr(keep(col_major(p.longitudinal_hamiltonian)))
+        fx, fz = keep(p.transverse_field), keep(p.longitudinal_field)
+        d.transverse_field, d.transverse_field_size = _dptr(fx), fx.size
+        d.longitudinal_field, d.longitudinal_field_size = _dptr(fz), fz.size
+        d.integration_time = float(p.integration_time)
+        d.minimum_field_change = float(p.minimum_field_change)
+    else:
+        d.hamiltonian = _dptr(keep(col_major(p.time_indepenent_hamiltonian)))
     d.initial_density_matrix = _dptr(keep(col_major(p.initial_density_matrix)))
     d.gamma = _dptr(keep(p.gamma))
     d.lambda_ = _dptr(keep(p.lambda_))
@@ -256,6 +266,12 @@ class Hierarchy:
         out = np.zeros(2 * nb * self.n * self.n, np.float64)
         self._check(self.lib.phi_gpu_get_time_local(self.ctx, out.ctypes.data))
         return out.view(np.complex128).reshape(nb, self.n, self.n)
+
+    def hamiltonian(self) -> np.ndarray:
+        """The Hamiltonian the next stage starts from (N x N complex)."""
+        out = np.zeros(2 * self.n * self.n, np.float64)
+        self._check(self.lib.phi_gpu_get_hamiltonian(self.ctx, out.ctypes.data))
+        return from_col_major(out, self.n)
 
     def rho0(self) -> np.ndarray:
         out = np.zeros(2 * self.n * self.n, np.float64)

@@ -128,3 +128,25 @@ def random_hermitian_state(M: int, n: int, seed: int = 1) -> np.ndarray:
     A = rng.normal(size=(M, n, n)) + 1j * rng.normal(size=(M, n, n))
     A = (A + np.conj(np.transpose(A, (0, 2, 1)))) / 2
     return np.ascontiguousarray(np.transpose(A, (0, 2, 1))).view(np.float64).reshape(-1).copy()
+
+
+def annealed(p: PhiParameters, t_end: float, seed: int = 0, samples: int = 5, complex_x: bool = False,
+             min_field_change: float = 0.01) -> PhiParameters:
+    """The same problem with an annealing Hamiltonian: H_X = the off-diagonal
+    part of H (times a phase when complex_x), H_Z = its diagonal, seeded field
+    samples ramping f_x 1 -> 0 and f_z 0 -> 1 over integration_time = t_end."""
+    rng = np.random.default_rng(seed)
+    H = np.asarray(p.time_indepenent_hamiltonian, np.complex128)
+    off = H - np.diag(np.diag(H))
+    if complex_x:
+        ph = np.exp(1j * rng.uniform(0, np.pi, size=off.shape))
+        off = np.triu(off * ph, 1)
+        off = off + off.conj().T
+    p.time_indepenent_hamiltonian = None
+    p.transverse_hamiltonian = off
+    p.longitudinal_hamiltonian = np.diag(np.diag(H)).astype(np.complex128)
+    p.transverse_field = np.linspace(1.0, 0.0, samples) + 0.1 * rng.normal(size=samples)
+    p.longitudinal_field = np.linspace(0.0, 1.0, samples) + 0.1 * rng.normal(size=samples)
+    p.integration_time = t_end
+    p.minimum_field_change = min_field_change
+    return p

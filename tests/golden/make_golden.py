@@ -37,7 +37,14 @@ Outputs (committed; the GPU host has no reference tree):
                         with (RK4 never stores them: PHI writes zeros there)
 
     python tests/golden/make_golden.py /root/reference filter    # filtering fixture only
+  ref_anneal.json       annealing Hamiltonians (TransverseHamiltonian /
+                        LongitudinalHamiltonian and their fields): per case,
+                        rho_0 with %.17g and, for small hierarchies, the whole
+                        final state from the restart file (the reference build
+                        runs them with its LAPACK shim's tridiagonal solve)
+
     python tests/golden/make_golden.py /root/reference timelocal # time-local fixture only
+    python tests/golden/make_golden.py /root/reference anneal    # annealing fixture only
 """
 from __future__ import annotations
 
@@ -270,6 +277,61 @@ def make_timelocal_fixture():
         json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
 
 
+# (case id, builder, builder kwargs, annealed() kwargs, method, timestep, t_end, TimeLocal)
+ANNEAL_CASES = [
+    ("indep_n3_k2_t3/rk4", "random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2),
+     dict(seed=1), "rk4", 0.001, 0.05, False),
+    ("indep_n3_k2_t3/rkf45", "random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2),
+     dict(seed=1), "rkf45", 0.001, 0.05, False),
+    ("indep_n3_k2_t3_complex/rk4", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2), dict(seed=2, complex_x=True), "rk4",
+     0.001, 0.05, False),
+    ("indep_n3_k2_t3_gate0.2/rk4", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2), dict(seed=3, min_field_change=0.2),
+     "rk4", 0.001, 0.05, False),
+    ("indep_n3_k2_t3_timelocal/rkf45", "random_problem",
+     dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2), dict(seed=1), "rkf45", 0.001, 0.05, True),
+    ("diag_n4_k2_t3/rk4", "random_problem", dict(kind="diagonal", n=4, matsubara=2, truncation=3, seed=3),
+     dict(seed=1), "rk4", 0.001, 0.05, False),
+    ("full_n3_k2_t3/rkf45", "random_problem", dict(kind="full", n=3, matsubara=2, truncation=3, seed=3),
+     dict(seed=4), "rkf45", 0.001, 0.05, False),
+    ("frenkel7_L2/rkf45", "config:frenkel7", dict(depth=2), dict(seed=1), "rkf45", 0.001, 0.05, False),
+]
+
+
+def make_anneal_fixture():
+    outs = []
+    for cid, builder, kw, akw, method, dt, t_end, tl in ANNEAL_CASES:
+        p = cases.annealed(build(builder, kw), t_end, **akw)
+        p.use_time_local_truncation = tl
+        if method == "rkf45":
+            p.fix_incompatible_combinations("rkf45")
+        n = p.num_states
+        with tempfile.TemporaryDirectory() as d:
+            prm, out, rst, rho_f = (os.path.join(d, x) for x in ("in.prm", "out.txt", "restart.txt", "rho.txt"))
+            with open(prm, "w") as f:
+                f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_file=out)
+                        + f"RestartFile={rst}\nRestartOutputTimeSecs=1\n")
+            try:
+                subprocess.run([O.REF_DRIVER, "run", prm, method, "1", rho_f], check=True, timeout=120,
+                               stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            except subprocess.TimeoutExpired:
+                print(f"{cid}: TIMEOUT", flush=True)
+                continue
+            rho = O.parse_rho_file(rho_f, n)
+            numbers = parse_restart_state(open(rst).read(), n)
+        M = O.node_count(p.num_bath_couplings * p.num_matsubara_terms, p.hierarchy_truncation_level)
+        case = {"id": cid, "builder": builder, "kwargs": kw, "anneal": akw, "method": method, "timestep": dt,
+                "t_end": t_end, "time_local": tl, "num_nodes": M,
+                "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}
+        if M <= 100:
+            case["state_6_digits"] = numbers[:M * n * n]
+        outs.append(case)
+        print(f"{cid}: M={M}", flush=True)
+    with open(os.path.join(HERE, "ref_anneal.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
@@ -286,10 +348,14 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "timelocal":
         make_timelocal_fixture()
         return
+    if len(sys.argv) > 2 and sys.argv[2] == "anneal":
+        make_anneal_fixture()
+        return
     make_restart_fixture()
     make_output_fixture()
     make_filter_fixture()
     make_timelocal_fixture()
+    make_anneal_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)
