@@ -292,21 +292,35 @@ PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
 /* ---- Restart files --------------------------------------------------------
  * PHI's restart layout (RestartHelper::WriteRestartFile / ReadRestartFile,
  * restart_helper.cc:30-84): the time, the step size, then one line per node
- * with its N*N elements in storage order as "(re,im)".  Written with 17
- * significant digits (PHI writes 6); read in either form.  Files that also
- * hold time-local truncation matrices are rejected.  The host functions work
- * on host buffers of 2*M*N*N doubles and need no GPU. */
+ * with its N*N elements in storage order as "(re,im)", and for a time-local
+ * run one more line per (bath m, term k) with the stored Q_{m,k}.  Written
+ * with 17 significant digits (PHI writes 6); read in either form.  The host
+ * functions work on host buffers (2*M*N*N doubles of state, 2*N*N doubles
+ * per extra matrix) and need no GPU.  phi_restart_read_file /
+ * phi_restart_write_file handle files without extra matrices (a file with
+ * more values is rejected); the _ex forms read / write exactly
+ * num_matrices of them after the nodes. */
 PHI_API int phi_restart_read_file(const char *path, int32_t num_states, int64_t num_nodes, double *state,
                                   double *time, double *timestep);
 PHI_API int phi_restart_write_file(const char *path, int32_t num_states, int64_t num_nodes, const double *state,
                                    double time, double timestep);
+PHI_API int phi_restart_read_file_ex(const char *path, int32_t num_states, int64_t num_nodes, double *state,
+                                     double *time, double *timestep, double *matrices, int64_t num_matrices);
+PHI_API int phi_restart_write_file_ex(const char *path, int32_t num_states, int64_t num_nodes,
+                                      const double *state, double time, double timestep,
+                                      const double *matrices, int64_t num_matrices);
 PHI_API int phi_restart_last_error(char *buf, size_t len);
 /* The context's state and time to / from a restart file (RestartInput and
- * RestartFile of PHI's parameter file). */
+ * RestartFile of PHI's parameter file).  A time-local context writes its
+ * stored Q_{m,k} after the nodes (zero after RK4, which never stores them,
+ * as in PHI) and reads them back as PHI's Initialize does
+ * (hierarchy_integrator.cc:1046-1068: Q_m = sum_k Q_{m,k}, then restored). */
 PHI_API int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double timestep);
 PHI_API int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *timestep);
-/* Binary fast path: "PHIB200S", uint32 version 1, uint32 N, int64 M, double
- * time, double step size, then the 2*M*N*N doubles of the state. */
+/* Binary fast path: "PHIB200S", uint32 version, uint32 N, int64 M, double
+ * time, double step size, the 2*M*N*N doubles of the state; version 2 adds
+ * an int64 count of time-local matrices and their 2*N*N doubles each
+ * (written by time-local contexts; version 1 files load as count 0). */
 PHI_API int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timestep);
 PHI_API int phi_gpu_load_state(phi_ctx *ctx, const char *path, double *timestep);
 

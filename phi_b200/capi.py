@@ -142,6 +142,10 @@ SIGNATURES = [
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
     ("phi_restart_read_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, POINTER(c_double), POINTER(c_double)]),
     ("phi_restart_write_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, c_double, c_double]),
+    ("phi_restart_read_file_ex", c_int, [c_char_p, c_int32, c_int64, c_void_p, POINTER(c_double),
+                                         POINTER(c_double), c_void_p, c_int64]),
+    ("phi_restart_write_file_ex", c_int, [c_char_p, c_int32, c_int64, c_void_p, c_double, c_double, c_void_p,
+                                          c_int64]),
     ("phi_restart_last_error", c_int, [c_char_p, c_size_t]),
     ("phi_gpu_write_restart", c_int, [c_void_p, c_char_p, c_double]),
     ("phi_gpu_read_restart", c_int, [c_void_p, c_char_p, POINTER(c_double)]),

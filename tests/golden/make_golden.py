@@ -44,7 +44,17 @@ Outputs (committed; the GPU host has no reference tree):
                         runs them with its LAPACK shim's tridiagonal solve)
 
     python tests/golden/make_golden.py /root/reference timelocal # time-local fixture only
+  ref_restart_timelocal_n3.txt / .json
+                        a restart file the reference build wrote at t1 of an
+                        RKF45 time-local run (nodes, then the stored Q_{m,k}),
+                        and rho_0 (%.17g) of the reference restarted from it
+                        (RestartInput) to t2.  PHI writes the step size after
+                        its last-step clamp, 0, and a run restarted with it
+                        never advances, so the step-size line is replaced by
+                        the run's timestep before the restart
+
     python tests/golden/make_golden.py /root/reference anneal    # annealing fixture only
+    python tests/golden/make_golden.py /root/reference restart_tl # time-local restart fixture only
 """
 from __future__ import annotations
 
@@ -332,6 +342,45 @@ def make_anneal_fixture():
         json.dump({"generator": "tests/golden/make_golden.py", "cases": outs}, f, indent=0)
 
 
+RESTART_TL_CASE = ("random_problem", dict(kind="independent", n=3, matsubara=2, truncation=3, seed=2),
+                   0.001, 0.02, 0.04)
+
+
+def make_restart_tl_fixture():
+    builder, kw, dt, t1, t2 = RESTART_TL_CASE
+    p = build(builder, kw)
+    p.use_time_local_truncation = True
+    p.fix_incompatible_combinations("rkf45")
+    n = p.num_states
+    with tempfile.TemporaryDirectory() as d:
+        prm1, prm2, out, rst, rho1, rho2 = (os.path.join(d, x) for x in
+                                            ("a.prm", "b.prm", "o.txt", "restart.txt", "r1.txt", "r2.txt"))
+        with open(prm1, "w") as f:
+            f.write(O.param_file_text(p, timestep=dt, t_end=t1, output_file=out)
+                    + f"RestartFile={rst}\nRestartOutputTimeSecs=1\n")
+        subprocess.run([O.REF_DRIVER, "run", prm1, "rkf45", "1", rho1], check=True, timeout=120,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        lines = open(rst).read().split("\n")
+        lines[1] = repr(float(dt))  # PHI wrote the clamped step size (0)
+        text = "\n".join(lines)
+        with open(rst, "w") as f:
+            f.write(text)
+        with open(prm2, "w") as f:
+            f.write(O.param_file_text(p, timestep=dt, t_end=t2, output_file=out) + f"RestartInput={rst}\n")
+        subprocess.run([O.REF_DRIVER, "run", prm2, "rkf45", "1", rho2], check=True, timeout=120,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        rho = O.parse_rho_file(rho2, n)
+    with open(os.path.join(HERE, "ref_restart_timelocal_n3.txt"), "w") as f:
+        f.write(text)
+    with open(os.path.join(HERE, "ref_restart_timelocal_n3.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "builder": builder, "kwargs": kw,
+                   "method": "rkf45", "time_local": True, "timestep": dt, "t1": t1, "t2": t2,
+                   "num_matrices": p.num_bath_couplings * p.num_matsubara_terms,
+                   "edited": "step-size line set to the timestep (PHI writes the clamped 0)",
+                   "rho0_t2_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}, f, indent=0)
+    print("time-local restart fixture written", flush=True)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     if not O.ref_available():
@@ -351,11 +400,15 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "anneal":
         make_anneal_fixture()
         return
+    if len(sys.argv) > 2 and sys.argv[2] == "restart_tl":
+        make_restart_tl_fixture()
+        return
     make_restart_fixture()
     make_output_fixture()
     make_filter_fixture()
     make_timelocal_fixture()
     make_anneal_fixture()
+    make_restart_tl_fixture()
     golden = parse_reference_tests(ref_root)
     with open(os.path.join(HERE, "reference_tests.json"), "w") as f:
         json.dump({"source": "src/hierarchy_integrator_test.cc:350-509", "vectors": golden}, f, indent=1)

@@ -175,12 +175,9 @@ def test_set_state_resets_matrices_and_refusals(tmp_path):
         assert np.abs(h.time_local()).max() > 0
         h.set_state(s0)
         assert np.abs(h.time_local()).max() == 0
-        # PHI turns time-local truncation off for steady states; restart
-        # files here do not carry the Q matrices.
+        # PHI turns time-local truncation off for steady states.
         with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
             h.steady_state(tol=1e-10)
-        with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
-            h.write_restart(str(tmp_path / "r.txt"), 0.001)
 
 
 def test_parameter_file_time_local(tmp_path):
@@ -194,3 +191,59 @@ def test_parameter_file_time_local(tmp_path):
         h.rk4(0.001, 0.05)
         b = h.get_state()
     assert np.abs(a - b).max() <= 1e-14 * np.abs(b).max()
+
+
+RST = os.path.join(HERE, "golden", "ref_restart_timelocal_n3.txt")
+RST_META = json.load(open(os.path.join(HERE, "golden", "ref_restart_timelocal_n3.json")))
+
+
+def _rst_problem():
+    p = getattr(cases, RST_META["builder"])(**RST_META["kwargs"])
+    p.use_time_local_truncation = True
+    p.fix_incompatible_combinations("rkf45")
+    return p
+
+
+def test_continue_from_reference_restart_file():
+    """Read the reference's time-local restart file (nodes and stored Q_{m,k},
+    restored as PHI's Initialize does) and continue RKF45 to t2: rho_0 equals
+    the reference restarted from the same file."""
+    p = _rst_problem()
+    with Hierarchy(p) as h:
+        dt = h.read_restart(RST)
+        assert h.time == RST_META["t1"] and dt == RST_META["timestep"]
+        n, nb, K1 = p.num_states, p.num_bath_couplings, p.num_matsubara_terms
+        st = np.zeros(2 * h.num_nodes * n * n)
+        q = np.zeros(2 * nb * K1 * n * n)
+        t, d = ctypes.c_double(), ctypes.c_double()
+        assert h.lib.phi_restart_read_file_ex(RST.encode(), n, h.num_nodes, st.ctypes.data, ctypes.byref(t),
+                                              ctypes.byref(d), q.ctypes.data, nb * K1) == capi.PHI_OK
+        q_sum = q.view(np.complex128).reshape(nb, K1, n, n).sum(axis=1)
+        assert np.abs(h.time_local() - q_sum).max() <= 1e-15 * np.abs(q_sum).max()
+        h.rkf45(dt, RST_META["t2"], 1e-6, 1e-6)
+        rho = h.rho0()
+    ref = np.array([complex(a, b) for a, b in RST_META["rho0_t2_colmajor"]]).reshape(n, n).T
+    assert np.abs(rho - ref).max() <= FP64_TOL * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("fmt", ["text", "binary"])
+def test_restart_round_trip_keeps_matrices(tmp_path, fmt):
+    """A time-local context's restart (17 digits) or state file carries the
+    stored Q_{m,k}; a context loaded from it continues exactly as the one
+    that wrote it (after an accepted RKF45 step the stored and the current
+    matrices agree)."""
+    p = _rst_problem()
+    path = str(tmp_path / ("r.txt" if fmt == "text" else "r.bin"))
+    with Hierarchy(p) as a:
+        st = a.rkf45(0.001, 0.02, 1e-6, 1e-6)
+        (a.write_restart if fmt == "text" else a.save_state)(path, 0.001)
+        qa = a.time_local()
+        a.rkf45(0.001, 0.04, 1e-6, 1e-6)
+        end_a = a.get_state()
+    with Hierarchy(p) as b:
+        (b.read_restart if fmt == "text" else b.load_state)(path)
+        assert np.abs(b.time_local() - qa).max() <= 1e-15 * np.abs(qa).max()
+        b.rkf45(0.001, 0.04, 1e-6, 1e-6)
+        end_b = b.get_state()
+    assert st["accepted"] > 0
+    assert np.abs(end_a - end_b).max() <= 1e-13 * np.abs(end_a).max()
