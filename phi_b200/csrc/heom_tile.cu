@@ -23,7 +23,7 @@ __global__ void __launch_bounds__(kTileThreads, TileMinBlocks<KT, MIXED>::value)
 
 template <int N, int KT, bool MIXED>
 cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
-  using S = TileShape<N>;
+  using S = TileShape<N, MIXED>;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
   const size_t smem_max = tile_smem<N, MIXED>(p.c.T, kMaxPre, max_bytes);
   auto kern = heom_tile_kernel<N, KT, MIXED>;
@@ -157,8 +157,9 @@ cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
 
 namespace {
 template <int N>
-long long tiles_of(long long M) {
-  return (M + TileShape<N>::NT - 1) / TileShape<N>::NT;
+long long tiles_of(long long M, bool mixed) {
+  const long long nt = mixed ? TileShape<N, true>::NT : TileShape<N, false>::NT;
+  return (M + nt - 1) / nt;
 }
 template <int N>
 size_t stage_smem_n(const TileParams &p, bool mixed) {
@@ -166,19 +167,19 @@ size_t stage_smem_n(const TileParams &p, bool mixed) {
 }
 }  // namespace
 
-long long tile_count(const HeomConsts &c) {
+long long tile_count(const HeomConsts &c, bool mixed) {
   switch (c.N) {
-    case 2: return tiles_of<2>(c.M);
-    case 3: return tiles_of<3>(c.M);
-    case 4: return tiles_of<4>(c.M);
-    case 5: return tiles_of<5>(c.M);
-    case 6: return tiles_of<6>(c.M);
-    case 7: return tiles_of<7>(c.M);
-    case 8: return tiles_of<8>(c.M);
-    case 10: return tiles_of<10>(c.M);
-    case 12: return tiles_of<12>(c.M);
-    case 16: return tiles_of<16>(c.M);
-    case 24: return tiles_of<24>(c.M);
+    case 2: return tiles_of<2>(c.M, mixed);
+    case 3: return tiles_of<3>(c.M, mixed);
+    case 4: return tiles_of<4>(c.M, mixed);
+    case 5: return tiles_of<5>(c.M, mixed);
+    case 6: return tiles_of<6>(c.M, mixed);
+    case 7: return tiles_of<7>(c.M, mixed);
+    case 8: return tiles_of<8>(c.M, mixed);
+    case 10: return tiles_of<10>(c.M, mixed);
+    case 12: return tiles_of<12>(c.M, mixed);
+    case 16: return tiles_of<16>(c.M, mixed);
+    case 24: return tiles_of<24>(c.M, mixed);
     default: return -1;
   }
 }

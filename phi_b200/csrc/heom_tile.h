@@ -14,8 +14,8 @@ cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream);
 int mixed_node_stride(int N);
 
 // ---- batched stages over many hierarchies (heom_tile_batch.cu) ----
-// Tiles of one hierarchy (-1 when N has no tile kernel).
-long long tile_count(const HeomConsts &c);
+// Tiles of one hierarchy in the given arithmetic (-1 when N has no tile kernel).
+long long tile_count(const HeomConsts &c, bool mixed);
 // Dynamic shared memory of one tile of stage launch L.
 size_t tile_stage_smem(const StageLaunch &L);
 // Size and host image of the per-instance tile parameters of stage launch L.

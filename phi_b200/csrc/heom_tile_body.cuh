@@ -151,14 +151,18 @@ __device__ __forceinline__ double2 cfma(double2 acc, double2 b, double s) {
 }
 template <class TX> __device__ __forceinline__ void st_stream(TX *p, TX v) { __stcs(p, v); }
 
-template <int N>
+template <int N, bool MIXED>
 struct TileShape {
   static constexpr int E = N * N;
   static constexpr int EP = E + (E & 1);  // complex64 node stride (16-byte aligned nodes)
   static constexpr int P = N * (N + 1) / 2;
-  // About one (node, pair) item per thread; two for N >= 12, whose nodes
-  // would otherwise leave a tile of one node and idle threads.
-  static constexpr int NT0 = (N >= 12 ? 2 : 1) * kTileThreads / P;
+  // (node, pair) items per thread: two for N >= 12, whose nodes would
+  // otherwise leave a tile of one node and idle threads, and two in mixed
+  // precision from N = 4 (timed on B200: the 7-site RKF45 step 0.245 ->
+  // 0.238 ms, the batched workload +16 % throughput; from N = 2 it gains
+  // less, FP64 is 9 % slower with two, and three are slower in both
+  // arithmetics); one otherwise.
+  static constexpr int NT0 = ((N >= 12 || (MIXED && N >= 4)) ? 2 : 1) * kTileThreads / P;
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
   // Column stride of the derivative tile in shared memory: odd, so the
   // transposed (j, i) writes of one warp fall in distinct banks.
@@ -168,7 +172,7 @@ struct TileShape {
 
 template <int N, bool MIXED>
 struct TileLayout {
-  using S = TileShape<N>;
+  using S = TileShape<N, MIXED>;
   static constexpr int ES = MIXED ? S::EP : S::E;  // node stride of X / k buffers
   static constexpr int XB = MIXED ? 8 : 16;        // bytes per element of X / k
   // byte offsets in dynamic shared memory
@@ -227,7 +231,7 @@ static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, i
 template <int N, int KT, bool MIXED>
 __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
                                          uint32_t par0, uint32_t par1) {
-  using S = TileShape<N>;
+  using S = TileShape<N, MIXED>;
   using Lay = TileLayout<N, MIXED>;
   using TX = typename std::conditional<MIXED, float2, double2>::type;
   using R = typename std::conditional<MIXED, float, double>::type;
@@ -638,7 +642,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
 
 template <int N, bool MIXED>
 inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
-  using S = TileShape<N>;
+  using S = TileShape<N, MIXED>;
   using Lay = TileLayout<N, MIXED>;
   size_t b = Lay::kPre;
   for (int i = 0; i < npre; ++i)

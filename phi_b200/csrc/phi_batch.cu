@@ -69,7 +69,7 @@ struct phi_batch {
       std::stable_sort(idx.begin(), idx.end(), [&](int a, int b) {
         const phi::HeomConsts &ca = inst[a]->c, &cb = inst[b]->c;
         if (ca.N != cb.N) return ca.N > cb.N;
-        return phi::tile_count(ca) > phi::tile_count(cb);
+        return phi::tile_count(ca, inst[a]->mixed()) > phi::tile_count(cb, inst[b]->mixed());
       });
     }
     return idx;
@@ -124,7 +124,7 @@ int build_plan(phi_batch *b, int st, double dt, int order, StagePlan *sp) {
   for (size_t k = 0; k < idx.size(); ++k) {
     const phi::StageLaunch L = stage_launch(b->inst[idx[k]], st, dt);
     phi::tile_params_host(L, params.data() + k * pb);
-    start[k + 1] = start[k] + phi::tile_count(L.c);
+    start[k + 1] = start[k] + phi::tile_count(L.c, L.mixed);
     smem = std::max(smem, phi::tile_stage_smem(L));
   }
   if (!sp->params.ptr || sp->params.bytes < params.size()) {
