@@ -185,12 +185,12 @@ struct TileLayout {
 };
 
 // CTAs per SM the register budget is fitted to (timed on c2, 7 sites, K+1 = 2:
-// mixed runs 10 % faster at 5 CTAs with a few spilled registers, FP64 6 %
-// faster at 4 without spills); more neighbour terms per site keep more
-// gathered values live.
+// FP64 6 % faster at 4 CTAs than at 5 without spills; mixed, with its two
+// items per thread, 1 % faster at 4 (64 registers) than at 5 and 4 % faster
+// than at 3); more neighbour terms per site keep more gathered values live.
 template <int KT, bool MIXED>
 struct TileMinBlocks {
-  static constexpr int warps = KT == 1 ? 40 : (KT == 2 ? (MIXED ? 40 : 32) : 24);  // resident warps per SM
+  static constexpr int warps = KT == 1 ? 40 : (KT == 2 ? 32 : 24);  // resident warps per SM
   static constexpr int value = warps / kTileWarps;
 };
 
