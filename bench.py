@@ -397,6 +397,26 @@ def run_steady(args):
     print(json.dumps(out), flush=True)
 
 
+def dgemm_peak_tflops(n: int = 8192, reps: int = 5) -> float:
+    """Measured FP64 matrix-multiply rate of this GPU (cuBLAS DGEMM through
+    torch.matmul on float64), 2 n^3 flops per product, best of reps."""
+    import torch
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    c = torch.matmul(a, b)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b, out=c)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    del a, b, c
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
 def main():
     global WORKLOAD, T_END
     args = parse_args()
@@ -599,6 +619,19 @@ def main():
             "gpu_launches": ((steps_done + 15) // 16) * 16 * 7,
             "clocks": clocks,
         }
+        if WORKLOAD == "ring24":
+            # N = 24 sits near the FP64 ridge: the FP64 path's compute
+            # roofline, 8 N^3 flops per node apply (one complex N x N
+            # product), against the measured FP64 GEMM rate of this GPU.
+            fp64_ms = ms_per_step if prec == capi.PHI_PREC_FP64 else other_ms_per_step
+            fp64_applies = 6 * M / (fp64_ms / 1e3)
+            flops = 8 * N ** 3
+            dpeak = dgemm_peak_tflops()
+            ach = fp64_applies * flops / 1e12
+            out["fp64_compute_roofline"] = {
+                "achieved_tflops": ach, "peak_tflops": dpeak, "frac": ach / dpeak,
+                "flops_per_apply": flops, "node_applies_per_s": fp64_applies,
+                "peak_kind": "measured: cuBLAS DGEMM 8192^3 (torch.matmul float64), best of 5"}
         if not args.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline_port(p)
         print(json.dumps(out), flush=True)
