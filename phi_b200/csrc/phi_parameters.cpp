@@ -510,6 +510,13 @@ void PhiParameters::Write(std::ofstream *out, long long num_matrices) {
   };
   row("gamma", gamma, num_bath_couplings);
   row("lambda", lambda, num_bath_couplings);
+  row("TransverseField", initial_hamiltonian_field, initial_hamiltonian_field_size);
+  row("LongitudinalField", final_hamiltonian_field, final_hamiltonian_field_size);
+  if (is_multiple_independent_baths && multiple_independent_bath_indices && num_bath_couplings > 0) {
+    o << "#multiBath:\n#";
+    for (int i = 0; i < num_bath_couplings; ++i)
+      o << multiple_independent_bath_indices[i] << (i + 1 < num_bath_couplings ? "," : "\n");
+  }
   if (bath_coupling_op) {
     const int width = is_full_bath_coupling ? num_states * num_states : num_states;
     o << (is_full_bath_coupling ? "#FullBathTerms:\n" : "#CorrelatedCouplingTerms:\n");
@@ -530,6 +537,8 @@ void PhiParameters::Write(std::ofstream *out, long long num_matrices) {
       o << m[(size_t)(r + 1) * num_states - 1] << "\n";
     }
   };
+  matrix("TransverseHamiltonian", initial_annealing_hamiltonian);
+  matrix("LongitudinalHamiltonian", final_annealing_hamiltonian);
   matrix("Hamiltonian", time_indepenent_hamiltonian);
   matrix("InitialDensityMatrix", initial_density_matrix);
   if (!restart_input_filename.empty()) o << "#RestartInput=" << restart_input_filename << "\n";

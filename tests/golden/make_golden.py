@@ -155,24 +155,37 @@ OUTPUT_CASE = ("random_problem", dict(kind="independent", n=3, matsubara=2, trun
                0.002)
 
 
+# (file stem, annealed() kwargs or None, TimeLocal, FilterTolerance)
+OUTPUT_VARIANTS = [("ref_output_indep_n3_rk4", None, False, 0.0),
+                   ("ref_output_anneal_n3_rk4", dict(seed=1), True, 1e-3)]
+
+
 def make_output_fixture():
     builder, kw, dt, t_end, out_step = OUTPUT_CASE
-    p = build(builder, kw)
     phi_bin = os.path.join(os.path.dirname(O.REF_DRIVER), "phi")
-    with tempfile.TemporaryDirectory() as d:
-        prm, out = os.path.join(d, "in.prm"), os.path.join(d, "out.txt")
-        with open(prm, "w") as f:
-            f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_min_step=out_step, output_file=out)
-                    .replace("verbose=-2", "verbose=0"))
-        subprocess.run([phi_bin, prm, "rk4", "1"], check=True, timeout=120, stdout=subprocess.DEVNULL,
-                       stderr=subprocess.DEVNULL)
-        text = open(out).read()
-    with open(os.path.join(HERE, "ref_output_indep_n3_rk4.txt"), "w") as f:
-        f.write(text)
-    with open(os.path.join(HERE, "ref_output_indep_n3_rk4.json"), "w") as f:
-        json.dump({"generator": "tests/golden/make_golden.py", "builder": builder, "kwargs": kw,
-                   "method": "rk4", "timestep": dt, "t_end": t_end, "output_min_step": out_step}, f, indent=0)
-    print("output fixture written", flush=True)
+    for stem, akw, tl, ft in OUTPUT_VARIANTS:
+        p = build(builder, kw)
+        if akw is not None:
+            p = cases.annealed(p, t_end, **akw)
+        p.use_time_local_truncation = tl
+        p.filter_tolerance = ft
+        with tempfile.TemporaryDirectory() as d:
+            prm, out = os.path.join(d, "in.prm"), os.path.join(d, "out.txt")
+            with open(prm, "w") as f:
+                f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_min_step=out_step, output_file=out)
+                        .replace("verbose=-2", "verbose=0"))
+            subprocess.run([phi_bin, prm, "rk4", "1"], check=True, timeout=120, stdout=subprocess.DEVNULL,
+                           stderr=subprocess.DEVNULL)
+            text = open(out).read()
+        with open(os.path.join(HERE, stem + ".txt"), "w") as f:
+            f.write(text)
+        meta = {"generator": "tests/golden/make_golden.py", "builder": builder, "kwargs": kw,
+                "method": "rk4", "timestep": dt, "t_end": t_end, "output_min_step": out_step}
+        if akw is not None or tl or ft:
+            meta.update({"anneal": akw, "time_local": tl, "filter_tolerance": ft})
+        with open(os.path.join(HERE, stem + ".json"), "w") as f:
+            json.dump(meta, f, indent=0)
+        print(f"output fixture {stem} written", flush=True)
 
 
 # (case id, builder, builder kwargs, method, timestep, t_end, FilterTolerance)

@@ -86,17 +86,24 @@ def test_cli_steady_state_output_file(tmp_path):
     np.testing.assert_allclose(_complexes(final), rho_ref.T.reshape(-1), rtol=1e-5, atol=1e-6)
 
 
-def test_cli_output_file_matches_reference_layout(tmp_path):
+@pytest.mark.parametrize("stem", ["ref_output_indep_n3_rk4", "ref_output_anneal_n3_rk4"],
+                         ids=["static", "annealing_timelocal_filter"])
+def test_cli_output_file_matches_reference_layout(tmp_path, stem):
     """Our CLI's output file against the one the reference's `phi` wrote for
-    the same parameters (tests/golden/ref_output_indep_n3_rk4.txt): the same
-    '#' header lines (memory figures are each implementation's own), the same
-    dynamics-row times and values to PHI's 6 significant digits, the same
-    closing step count and the final row to its 4 digits."""
+    the same parameters (tests/golden/<stem>.txt; the second run anneals
+    with time-local truncation and filtering on): the same '#' header lines
+    (memory figures are each implementation's own), the same dynamics-row
+    times and values to PHI's 6 significant digits, the same closing step
+    count and the final row to its 4 digits."""
     import json as _json
     here = os.path.dirname(os.path.abspath(__file__))
-    meta = _json.load(open(os.path.join(here, "golden", "ref_output_indep_n3_rk4.json")))
-    ref_lines = open(os.path.join(here, "golden", "ref_output_indep_n3_rk4.txt")).read().splitlines()
+    meta = _json.load(open(os.path.join(here, "golden", stem + ".json")))
+    ref_lines = open(os.path.join(here, "golden", stem + ".txt")).read().splitlines()
     p = getattr(cases, meta["builder"])(**meta["kwargs"])
+    if meta.get("anneal") is not None:
+        p = cases.annealed(p, meta["t_end"], **meta["anneal"])
+    p.use_time_local_truncation = bool(meta.get("time_local", False))
+    p.filter_tolerance = float(meta.get("filter_tolerance", 0.0))
     out = tmp_path / "out.txt"
     path = _write(tmp_path, O.param_file_text(p, timestep=meta["timestep"], t_end=meta["t_end"],
                                               output_min_step=meta["output_min_step"], output_file=str(out))
