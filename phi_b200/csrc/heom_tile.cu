@@ -23,9 +23,9 @@ __global__ void __launch_bounds__(kTileThreads, TileMinBlocks<KT, MIXED>::value)
 
 template <int N, int KT, bool MIXED>
 cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
-  using S = TileShape<N, MIXED>;
+  using S = TileShape<N, MIXED, KT>;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
-  const size_t smem_max = tile_smem<N, MIXED>(p.c.T, kMaxPre, max_bytes);
+  const size_t smem_max = tile_smem<N, KT, MIXED>(p.c.T, kMaxPre, max_bytes);
   auto kern = heom_tile_kernel<N, KT, MIXED>;
   static thread_local int configured = -1;
   if (smem_max > 48 * 1024 && configured < (int)smem_max) {
@@ -34,7 +34,7 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
     configured = (int)smem_max;
   }
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
-  kern<<<(unsigned)tiles, kTileThreads, tile_smem<N, MIXED>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
+  kern<<<(unsigned)tiles, kTileThreads, tile_smem<N, KT, MIXED>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -156,30 +156,44 @@ cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
 }
 
 namespace {
-template <int N>
-long long tiles_of(long long M, bool mixed) {
-  const long long nt = mixed ? TileShape<N, true>::NT : TileShape<N, false>::NT;
+template <int N, int KT>
+long long tiles_of_k(long long M, bool mixed) {
+  const long long nt = mixed ? TileShape<N, true, KT>::NT : TileShape<N, false, KT>::NT;
   return (M + nt - 1) / nt;
 }
 template <int N>
+long long tiles_of(long long M, bool mixed, int K1) {
+  switch (K1) {
+    case 1: return tiles_of_k<N, 1>(M, mixed);
+    case 2: return tiles_of_k<N, 2>(M, mixed);
+    case 3: return tiles_of_k<N, 3>(M, mixed);
+    default: return -1;
+  }
+}
+template <int N>
 size_t stage_smem_n(const TileParams &p, bool mixed) {
-  return mixed ? tile_smem<N, true>(p.c.T, p.npre, p.pre_bytes) : tile_smem<N, false>(p.c.T, p.npre, p.pre_bytes);
+  switch (p.c.K1) {
+    case 1: return mixed ? tile_smem<N, 1, true>(p.c.T, p.npre, p.pre_bytes) : tile_smem<N, 1, false>(p.c.T, p.npre, p.pre_bytes);
+    case 2: return mixed ? tile_smem<N, 2, true>(p.c.T, p.npre, p.pre_bytes) : tile_smem<N, 2, false>(p.c.T, p.npre, p.pre_bytes);
+    case 3: return mixed ? tile_smem<N, 3, true>(p.c.T, p.npre, p.pre_bytes) : tile_smem<N, 3, false>(p.c.T, p.npre, p.pre_bytes);
+    default: return 0;
+  }
 }
 }  // namespace
 
 long long tile_count(const HeomConsts &c, bool mixed) {
   switch (c.N) {
-    case 2: return tiles_of<2>(c.M, mixed);
-    case 3: return tiles_of<3>(c.M, mixed);
-    case 4: return tiles_of<4>(c.M, mixed);
-    case 5: return tiles_of<5>(c.M, mixed);
-    case 6: return tiles_of<6>(c.M, mixed);
-    case 7: return tiles_of<7>(c.M, mixed);
-    case 8: return tiles_of<8>(c.M, mixed);
-    case 10: return tiles_of<10>(c.M, mixed);
-    case 12: return tiles_of<12>(c.M, mixed);
-    case 16: return tiles_of<16>(c.M, mixed);
-    case 24: return tiles_of<24>(c.M, mixed);
+    case 2: return tiles_of<2>(c.M, mixed, c.K1);
+    case 3: return tiles_of<3>(c.M, mixed, c.K1);
+    case 4: return tiles_of<4>(c.M, mixed, c.K1);
+    case 5: return tiles_of<5>(c.M, mixed, c.K1);
+    case 6: return tiles_of<6>(c.M, mixed, c.K1);
+    case 7: return tiles_of<7>(c.M, mixed, c.K1);
+    case 8: return tiles_of<8>(c.M, mixed, c.K1);
+    case 10: return tiles_of<10>(c.M, mixed, c.K1);
+    case 12: return tiles_of<12>(c.M, mixed, c.K1);
+    case 16: return tiles_of<16>(c.M, mixed, c.K1);
+    case 24: return tiles_of<24>(c.M, mixed, c.K1);
     default: return -1;
   }
 }

@@ -151,18 +151,21 @@ __device__ __forceinline__ double2 cfma(double2 acc, double2 b, double s) {
 }
 template <class TX> __device__ __forceinline__ void st_stream(TX *p, TX v) { __stcs(p, v); }
 
-template <int N, bool MIXED>
+template <int N, bool MIXED, int KT>
 struct TileShape {
   static constexpr int E = N * N;
   static constexpr int EP = E + (E & 1);  // complex64 node stride (16-byte aligned nodes)
   static constexpr int P = N * (N + 1) / 2;
   // (node, pair) items per thread: two for N >= 12, whose nodes would
-  // otherwise leave a tile of one node and idle threads, and two in mixed
+  // otherwise leave a tile of one node and idle threads, two in mixed
   // precision from N = 4 (timed on B200: the 7-site RKF45 step 0.245 ->
   // 0.238 ms, the batched workload +16 % throughput; from N = 2 it gains
-  // less, FP64 is 9 % slower with two, and three are slower in both
-  // arithmetics); one otherwise.
-  static constexpr int NT0 = ((N >= 12 || (MIXED && N >= 4)) ? 2 : 1) * kTileThreads / P;
+  // less, three are slower in both arithmetics), and two in FP64 for
+  // K+1 = 3 up to N = 6 (the 4-site steady solve -4.5 %; with K+1 <= 2 FP64
+  // is slower with two: 9 % on the 7-site step, 5 % on the batched one);
+  // one otherwise.
+  static constexpr bool kTwo = N >= 12 || (MIXED && N >= 4) || (!MIXED && KT == 3 && N <= 6);
+  static constexpr int NT0 = (kTwo ? 2 : 1) * kTileThreads / P;
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
   // Column stride of the derivative tile in shared memory: odd, so the
   // transposed (j, i) writes of one warp fall in distinct banks.
@@ -170,9 +173,9 @@ struct TileShape {
   static constexpr int EU = N * NP;
 };
 
-template <int N, bool MIXED>
+template <int N, bool MIXED, int KT>
 struct TileLayout {
-  using S = TileShape<N, MIXED>;
+  using S = TileShape<N, MIXED, KT>;
   static constexpr int ES = MIXED ? S::EP : S::E;  // node stride of X / k buffers
   static constexpr int XB = MIXED ? 8 : 16;        // bytes per element of X / k
   // byte offsets in dynamic shared memory
@@ -231,8 +234,8 @@ static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, i
 template <int N, int KT, bool MIXED>
 __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
                                          uint32_t par0, uint32_t par1) {
-  using S = TileShape<N, MIXED>;
-  using Lay = TileLayout<N, MIXED>;
+  using S = TileShape<N, MIXED, KT>;
+  using Lay = TileLayout<N, MIXED, KT>;
   using TX = typename std::conditional<MIXED, float2, double2>::type;
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES, NP = S::NP, EU = S::EU;
@@ -640,10 +643,10 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   return 0;
 }
 
-template <int N, bool MIXED>
+template <int N, int KT, bool MIXED>
 inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
-  using S = TileShape<N, MIXED>;
-  using Lay = TileLayout<N, MIXED>;
+  using S = TileShape<N, MIXED, KT>;
+  using Lay = TileLayout<N, MIXED, KT>;
   size_t b = Lay::kPre;
   for (int i = 0; i < npre; ++i)
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
