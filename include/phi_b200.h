@@ -285,6 +285,11 @@ PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);
 PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out, double dt,
                                      void *stream);
 
+/* Device memory of destroyed contexts is kept (up to 8 GiB) for the next
+ * allocation of the same size in this process; this returns it to the
+ * driver and gives the bytes released. */
+PHI_API int64_t phi_gpu_release_cached_memory(void);
+
 /* Copies the text of the last error on this context (or of the last failed
  * create when ctx is NULL) into buf. */
 PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);

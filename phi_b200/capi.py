@@ -124,6 +124,7 @@ SIGNATURES = [
     ("phi_gpu_get_active", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_time_local", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_get_hamiltonian", c_int, [c_void_p, c_void_p]),
+    ("phi_gpu_release_cached_memory", c_int64, []),
     ("phi_gpu_apply", c_int, [c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_apply_device", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_rk4", c_int, [c_void_p, c_double, c_double, c_double, c_void_p, c_void_p, c_int64,

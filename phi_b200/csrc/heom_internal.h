@@ -12,7 +12,14 @@
 
 namespace phi {
 
-// Owning device allocation.
+// Device / pinned host allocations reused across contexts of the process
+// (device_cache.cpp).
+cudaError_t cached_device_alloc(void **out, size_t bytes);
+void cached_device_free(void *p, size_t bytes);
+cudaError_t cached_host_alloc(void **out, size_t bytes);
+void cached_host_free(void *p, size_t bytes);
+
+// Owning device allocation (through the process-level cache).
 struct DeviceBuffer {
   void *ptr = nullptr;
   size_t bytes = 0;
@@ -37,7 +44,7 @@ struct DeviceBuffer {
   cudaError_t alloc(size_t n) {
     reset();
     if (n == 0) n = 16;
-    cudaError_t e = cudaMalloc(&ptr, n);
+    cudaError_t e = cached_device_alloc(&ptr, n);
     if (e != cudaSuccess) {
       ptr = nullptr;
       return e;
@@ -46,7 +53,7 @@ struct DeviceBuffer {
     return cudaSuccess;
   }
   void reset() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) cached_device_free(ptr, bytes);
     ptr = nullptr;
     bytes = 0;
   }

@@ -86,7 +86,7 @@ struct phi_ctx {
   double time = 0.0;
   std::string error;
   ~phi_ctx() {
-    if (host_ctl) cudaFreeHost(host_ctl);
+    if (host_ctl) phi::cached_host_free(host_ctl, sizeof(phi::Rkf45Ctl));
   }
 
   size_t state_bytes() const {

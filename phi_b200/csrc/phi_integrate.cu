@@ -339,7 +339,7 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
       return cudaSuccess;
     }, &ctx->rkf45_graph));
   }
-  if (!ctx->host_ctl) PHI_CK(cudaMallocHost(&ctx->host_ctl, sizeof(phi::Rkf45Ctl)));
+  if (!ctx->host_ctl) PHI_CK(phi::cached_host_alloc(&ctx->host_ctl, sizeof(phi::Rkf45Ctl)));
   phi::Rkf45Ctl *hpin = static_cast<phi::Rkf45Ctl *>(ctx->host_ctl);
   int result = PHI_OK;
   // Two graphs in flight: the done flag of launch j is read while launch j+1

@@ -188,7 +188,7 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     ctx->bicg_ell = ell;
   }
   phi::BicgScalars *host = nullptr;
-  PHI_SK(cudaMallocHost(&host, offsetof(phi::BicgScalars, partials)));
+  PHI_SK(phi::cached_host_alloc(reinterpret_cast<void **>(&host), offsetof(phi::BicgScalars, partials)));
   const long long max_graphs = (long long)max_steps / ((long long)ell * outer_per_graph) + 2;
   int result = PHI_OK;
   for (long long g = 0;; ++g) {
@@ -238,7 +238,7 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
       result = PHI_E_NO_CONVERGENCE;
     }
   }
-  cudaFreeHost(host);
+  phi::cached_host_free(host, offsetof(phi::BicgScalars, partials));
   if (result == PHI_OK || result == PHI_E_NO_CONVERGENCE) {
     const int flag = ctx->check_device_flag();
     if (flag != PHI_OK) result = flag;
