@@ -14,18 +14,31 @@ using namespace tile_detail;
 
 namespace {
 
+// Threads per CTA of the single-instance kernel: 320 for the 24-site mixed
+// kernel (a node's 300 pairs in one pass, two nodes per tile: timed on B200,
+// its RKF45 step 1.65 -> 1.56 ms), 256 otherwise (320 everywhere was slower
+// on the 7-site and the batched workloads).  The batched kernel always runs
+// 256, so its tile counts (tile_count) use that.
+template <int N, bool MIXED>
+struct TileBlock {
+  static constexpr int threads = (MIXED && N == 24) ? 320 : kTileThreads;
+};
+
 template <int N, int KT, bool MIXED>
-__global__ void __launch_bounds__(kTileThreads, TileMinBlocks<KT, MIXED>::value) heom_tile_kernel(TileParams p) {
+__global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
+                                  TileMinBlocks<KT, MIXED, TileBlock<N, MIXED>::threads>::value)
+    heom_tile_kernel(TileParams p) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   tile_init_barriers(smem_raw);
-  tile_body<N, KT, MIXED>(p, blockIdx.x, smem_raw, 0u, 0u);
+  tile_body<N, KT, MIXED, TileBlock<N, MIXED>::threads>(p, blockIdx.x, smem_raw, 0u, 0u);
 }
 
 template <int N, int KT, bool MIXED>
 cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
-  using S = TileShape<N, MIXED, KT>;
+  constexpr int BT = TileBlock<N, MIXED>::threads;
+  using S = TileShape<N, MIXED, KT, BT>;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
-  const size_t smem_max = tile_smem<N, KT, MIXED>(p.c.T, kMaxPre, max_bytes);
+  const size_t smem_max = tile_smem<N, KT, MIXED, BT>(p.c.T, kMaxPre, max_bytes);
   auto kern = heom_tile_kernel<N, KT, MIXED>;
   static thread_local int configured = -1;
   if (smem_max > 48 * 1024 && configured < (int)smem_max) {
@@ -34,7 +47,7 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
     configured = (int)smem_max;
   }
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
-  kern<<<(unsigned)tiles, kTileThreads, tile_smem<N, KT, MIXED>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
+  kern<<<(unsigned)tiles, BT, tile_smem<N, KT, MIXED, BT>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -151,7 +151,7 @@ __device__ __forceinline__ double2 cfma(double2 acc, double2 b, double s) {
 }
 template <class TX> __device__ __forceinline__ void st_stream(TX *p, TX v) { __stcs(p, v); }
 
-template <int N, bool MIXED, int KT>
+template <int N, bool MIXED, int KT, int BT = kTileThreads>
 struct TileShape {
   static constexpr int E = N * N;
   static constexpr int EP = E + (E & 1);  // complex64 node stride (16-byte aligned nodes)
@@ -165,7 +165,7 @@ struct TileShape {
   // is slower with two: 9 % on the 7-site step, 5 % on the batched one);
   // one otherwise.
   static constexpr bool kTwo = N >= 12 || (MIXED && N >= 4) || (!MIXED && KT == 3 && N <= 6);
-  static constexpr int NT0 = (kTwo ? 2 : 1) * kTileThreads / P;
+  static constexpr int NT0 = (kTwo ? 2 : 1) * BT / P;
   static constexpr int NT = NT0 < 1 ? 1 : (NT0 > 64 ? 64 : NT0);
   // Column stride of the derivative tile in shared memory: odd, so the
   // transposed (j, i) writes of one warp fall in distinct banks.
@@ -173,9 +173,9 @@ struct TileShape {
   static constexpr int EU = N * NP;
 };
 
-template <int N, bool MIXED, int KT>
+template <int N, bool MIXED, int KT, int BT = kTileThreads>
 struct TileLayout {
-  using S = TileShape<N, MIXED, KT>;
+  using S = TileShape<N, MIXED, KT, BT>;
   static constexpr int ES = MIXED ? S::EP : S::E;  // node stride of X / k buffers
   static constexpr int XB = MIXED ? 8 : 16;        // bytes per element of X / k
   // byte offsets in dynamic shared memory
@@ -191,10 +191,10 @@ struct TileLayout {
 // FP64 6 % faster at 4 CTAs than at 5 without spills; mixed, with its two
 // items per thread, 1 % faster at 4 (64 registers) than at 5 and 4 % faster
 // than at 3); more neighbour terms per site keep more gathered values live.
-template <int KT, bool MIXED>
+template <int KT, bool MIXED, int BT = kTileThreads>
 struct TileMinBlocks {
   static constexpr int warps = KT == 1 ? 40 : (KT == 2 ? 32 : 24);  // resident warps per SM
-  static constexpr int value = warps / kTileWarps;
+  static constexpr int value = warps / (BT / 32);
 };
 
 // New filter flags of a tile's nodes from |y_new|^2 staged in the first 8
@@ -204,9 +204,10 @@ struct TileMinBlocks {
 // wins the `>`, as in PHI's scan.  Kept out of line so its registers do not
 // add to the tile body's.
 static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, int slot, int N, int NP, int nt_here,
-                                               const uint8_t *act_in, uint8_t *act_out, double tol) {
+                                               const uint8_t *act_in, uint8_t *act_out, double tol,
+                                               int warps) {
   const int E = N * N, lane = threadIdx.x & 31;
-  for (int nd = threadIdx.x >> 5; nd < nt_here; nd += kTileWarps) {
+  for (int nd = threadIdx.x >> 5; nd < nt_here; nd += warps) {
     double m = 0.0;
     for (int w = lane; w < E; w += 32) {
       const int col = w / N;
@@ -231,11 +232,11 @@ static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, i
 // any copy was issued (RKF45 run finished), 0 when both barriers completed a
 // phase (barrier 1 with 0 bytes when p.npre == 0), -1 after a bounded wait gave up
 // (err_flag set; the caller must stop).
-template <int N, int KT, bool MIXED>
+template <int N, int KT, bool MIXED, int BT = kTileThreads>
 __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
                                          uint32_t par0, uint32_t par1) {
-  using S = TileShape<N, MIXED, KT>;
-  using Lay = TileLayout<N, MIXED, KT>;
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = TileLayout<N, MIXED, KT, BT>;
   using TX = typename std::conditional<MIXED, float2, double2>::type;
   using R = typename std::conditional<MIXED, float, double>::type;
   constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES, NP = S::NP, EU = S::EU;
@@ -269,7 +270,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
   double *coef = deph + NT;                                         // 24
   unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
-  R *cn = reinterpret_cast<R *>(wmax + kTileWarps);                          // NT*T |next prefactor|
+  R *cn = reinterpret_cast<R *>(wmax + (BT / 32));                          // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
   R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element
@@ -331,12 +332,12 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   const bool hreal = c.h_real;
   R *Hr = reinterpret_cast<R *>(Hs);
   if (hreal) {
-    for (int i = tid; i < E; i += kTileThreads) Hr[i] = (R)__ldg(c.H + i).x;
+    for (int i = tid; i < E; i += BT) Hr[i] = (R)__ldg(c.H + i).x;
   } else {
-    for (int i = tid; i < E; i += kTileThreads) Hs[i] = from_d2<TX>(__ldg(c.H + i));
+    for (int i = tid; i < E; i += BT) Hs[i] = from_d2<TX>(__ldg(c.H + i));
   }
-  for (int i = tid; i < E; i += kTileThreads) mats[i] = (R)__ldg(c.mats_elem + i);
-  for (int i = tid; i < P; i += kTileThreads) {
+  for (int i = tid; i < E; i += BT) mats[i] = (R)__ldg(c.mats_elem + i);
+  for (int i = tid; i < P; i += BT) {
     pi[i] = __ldg(c.pair_i + i);
     pj[i] = __ldg(c.pair_j + i);
   }
@@ -346,7 +347,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // input (-1 when absent), occupation, and the prefactor magnitudes for that
   // occupation, so the pair loop reads shared memory only.
   const uint8_t *act_in = c.filtered ? p.act[act_idx()] : nullptr;
-  for (int q = tid; q < tile_terms; q += kTileThreads) {
+  for (int q = tid; q < tile_terms; q += BT) {
     const int nd = q / T, t = q - nd * T;
     const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
     const int nt = __ldg(c.mi + n0 * T + q);
@@ -360,7 +361,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     cn[q] = (R)__ldg(c.sq_next + t * W + nt);
     cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
   }
-  for (int t = tid; t < T; t += kTileThreads) {
+  for (int t = tid; t < T; t += BT) {
     const double2 ct = __ldg(c.corr + t);
     ccr[2 * t] = (R)ct.x;
     ccr[2 * t + 1] = (R)ct.y;
@@ -382,7 +383,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // ---- phase 2: derivative of every (node, pair) ----
   const R ih = (R)c.inv_hbar;
   const int items = nt_here * P;
-  for (int it = tid; it < items; it += kTileThreads) {
+  for (int it = tid; it < items; it += BT) {
     const int nd = it / P, u = it - nd * P;
     const int i = pi[u], j = pj[u];
     const TX *X = Xs + nd * ES;
@@ -488,7 +489,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // pair loop above keeps its registers.  Item `it` maps to the thread that
   // wrote its two slots in the pair loop, so no barrier is needed before it.
   if (c.time_local) {
-    for (int it = tid; it < items; it += kTileThreads) {
+    for (int it = tid; it < items; it += BT) {
       const int nd = it / P, u = it - nd * P;
       const int i = pi[u], j = pj[u];
       if (i == j) continue;
@@ -526,7 +527,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   };
   if (p.mode == kModeApply) {
     TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += kTileThreads) {
+    for (int e = tid; e < tile_elems; e += BT) {
       const int nd = e / E, w = e - nd * E;
       st_stream(out + (n0 + nd) * ES + w, Us[uix(e)]);
     }
@@ -538,7 +539,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       const Rk4Ctl *rc = p.rk4;
       if (rc->out_factor > 0 && rc->step % rc->out_factor == 0 && rc->nout < rc->capacity) row = rc->nout;
     }
-    for (int e = tid; e < tile_elems; e += kTileThreads) {
+    for (int e = tid; e < tile_elems; e += BT) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const double2 kv = to_d2(Us[uix(e)]);
@@ -569,7 +570,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     const int s = p.stage;
     const double *cf = coef;
     TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += kTileThreads) {
+    for (int e = tid; e < tile_elems; e += BT) {
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const TX kx = Us[uix(e)];
@@ -626,7 +627,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       if (tid == 0) {
         unsigned long long m = wmax[0];
 #pragma unroll
-        for (int w = 1; w < kTileWarps; ++w) m = wmax[w] > m ? wmax[w] : m;
+        for (int w = 1; w < (BT / 32); ++w) m = wmax[w] > m ? wmax[w] : m;
         if (m) atomicMax(&p.ctl->err_bits, m);
       }
     }
@@ -638,20 +639,20 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     __syncthreads();
     const int ap = act_idx();
     tile_filter_flags(reinterpret_cast<const unsigned char *>(Us), (int)sizeof(TX), N, NP, nt_here,
-                      p.act[ap] + n0, p.act[ap ^ 1] + n0, c.filter_tol);
+                      p.act[ap] + n0, p.act[ap ^ 1] + n0, c.filter_tol, BT / 32);
   }
   return 0;
 }
 
-template <int N, int KT, bool MIXED>
+template <int N, int KT, bool MIXED, int BT = kTileThreads>
 inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
-  using S = TileShape<N, MIXED, KT>;
-  using Lay = TileLayout<N, MIXED, KT>;
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = TileLayout<N, MIXED, KT, BT>;
   size_t b = Lay::kPre;
   for (int i = 0; i < npre; ++i)
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
-  b += (size_t)(S::NT + 24 + kTileWarps) * sizeof(double);  // deph, coef, warp maxima
+  b += (size_t)(S::NT + 24 + BT / 32) * sizeof(double);  // deph, coef, warp maxima
   b += (size_t)(2 * S::NT * T + 2 * T + S::E) * Lay::XB / 2;  // cn, cp, ccr, mats in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;
