@@ -60,10 +60,17 @@ __device__ __forceinline__ int run_tile_any(const TileParams &p, long long tile,
   }
 }
 
-constexpr int kBatchMinBlocks = 24 / kTileWarps;  // 24 resident warps per SM
+// Resident CTAs per SM the register budget is fitted to: 4 in mixed
+// precision (64 registers), 3 in FP64 (timed on the 512-instance workload:
+// mixed 152 -> 145 ms per RK4 step at 4; FP64 229 ms at 3, 281 at 4; both
+// slower at 2).
+template <bool MIXED>
+struct BatchMinBlocks {
+  static constexpr int value = (MIXED ? 32 : 24) / kTileWarps;
+};
 
 template <bool MIXED>
-__global__ void __launch_bounds__(kTileThreads, kBatchMinBlocks)
+__global__ void __launch_bounds__(kTileThreads, BatchMinBlocks<MIXED>::value)
     heom_tile_batch_kernel(const TileParams *__restrict__ params, const long long *__restrict__ tile_start,
                            int count, long long total_tiles, int *err_flag) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
