@@ -187,13 +187,15 @@ struct TileLayout {
   static constexpr size_t kPre = kU + kUBytes;
 };
 
-// CTAs per SM the register budget is fitted to (timed on c2, 7 sites, K+1 = 2:
-// FP64 6 % faster at 4 CTAs than at 5 without spills; mixed, with its two
-// items per thread, 1 % faster at 4 (64 registers) than at 5 and 4 % faster
-// than at 3); more neighbour terms per site keep more gathered values live.
+// Resident warps per SM the register budget is fitted to (timed on B200).
+// K+1 = 2 (7 sites): FP64 6 % faster at 4 CTAs than at 5 without spills;
+// mixed, with its two items per thread, 1 % faster at 4 (64 registers) than
+// at 5 and 4 % faster than at 3.  K+1 = 1 (24 sites): FP64 1.6 % faster at
+// 4 CTAs than at 5; the 320-thread mixed kernel fastest at 4 CTAs (40
+// warps).  More neighbour terms per site keep more gathered values live.
 template <int KT, bool MIXED, int BT = kTileThreads>
 struct TileMinBlocks {
-  static constexpr int warps = KT == 1 ? 40 : (KT == 2 ? 32 : 24);  // resident warps per SM
+  static constexpr int warps = KT == 1 ? (MIXED ? 40 : 32) : (KT == 2 ? 32 : 24);
   static constexpr int value = warps / (BT / 32);
 };
 
