@@ -15,8 +15,9 @@
 //          input.  complex64 buffers pad every node to an even number of
 //          elements so each node range is 16-byte aligned.
 //
-// A CTA of kTileThreads threads owns a tile of NT consecutive nodes (about one
-// upper-triangle pair of one node per thread).  Everything the tile reads of
+// A CTA of BT threads (kTileThreads = 256, or what the single-instance
+// launch picks per (N, arithmetic)) owns a tile of NT consecutive nodes (one
+// or two upper-triangle pairs of one node per thread).  Everything the tile reads of
 // its own nodes is contiguous in HBM and arrives by TMA bulk copies issued at
 // CTA start:
 //
