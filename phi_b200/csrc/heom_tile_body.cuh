@@ -323,6 +323,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
 #pragma unroll
     for (int b = 0; b < kMaxPre; ++b) {
       if (b >= p.npre) break;
+      if (p.pre_bytes[b] == 0) continue;  // read from global in the epilogue
       const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
       if (b == 0 && p.mode == kModeRkf45) src = reinterpret_cast<const unsigned char *>(p.ybuf[ycur]);
       const int stride = p.pre_bytes[b] == 16 ? E : ES;
@@ -520,6 +521,11 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // element e of the tile: node nd = e / E, offset w = e % E; complex128
   // buffers are indexed (n0 + nd) * E + w, X / k buffers (n0 + nd) * ES + w.
   auto preD = [&](int b) { return reinterpret_cast<const double2 *>(PreBase + pre_off[b]); };
+  // The 24-site mixed kernel reads the RKF45 state y of stages 3-5 from global
+  // memory instead of staging it (a zero-byte operand slot): 18 KB less shared
+  // memory per tile, 3 CTAs per SM instead of 2 (c5 step 1.56 -> 1.52 ms; the
+  // same change was slower for 7 sites, whose CTA count it does not raise).
+  constexpr bool kYGlobal = MIXED && N == 24;
   auto preX = [&](int b) { return reinterpret_cast<const TX *>(PreBase + pre_off[b]); };
   double emax = 0.0;
   // Filtering: |y_new|^2 of element e goes to the first 8 bytes of its own
@@ -579,7 +585,8 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       const TX kx = Us[uix(e)];
       const double2 kv = to_d2(kx);
       if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; FP64 stage 0: y is the input
-        const double2 ys = (s == 0 && !MIXED) ? to_d2(Xs[nd * ES + w]) : preD(0)[e];
+        const double2 ys = (s == 0 && !MIXED) ? to_d2(Xs[nd * ES + w])
+                           : ((kYGlobal && p.pre_bytes[0] == 0) ? __ldg(p.ybuf[ycur] + gd) : preD(0)[e]);
         st_stream(static_cast<TX *>(p.k[s]) + gx, kx);
         const int row = s * (s + 1) / 2;
         double2 xv = ys;
@@ -589,7 +596,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         xv = cfma(xv, kv, cf[row + s]);
         out[gx] = from_d2<TX>(xv);
       } else {      // pre = {y, k0, k2, k3, k4}
-        const double2 ys = preD(0)[e];
+        const double2 ys = (kYGlobal && p.pre_bytes[0] == 0) ? __ldg(p.ybuf[ycur] + gd) : preD(0)[e];
         const double2 k0 = to_d2(preX(1)[nd * ES + w]), k2 = to_d2(preX(2)[nd * ES + w]);
         const double2 k3 = to_d2(preX(3)[nd * ES + w]), k4 = to_d2(preX(4)[nd * ES + w]);
         double2 y4 = cfma(ys, k0, cf[15]);
