@@ -158,8 +158,8 @@ TileParams tile_params_for(const StageLaunch &L) {
         p.pre_bytes[1 + r] = xb;
       }
     }
-    // 24-site mixed: stages 3-5 read y from global (see tile_body).
-    if (mixed && L.c.N == 24 && L.stage >= 3) p.pre_bytes[0] = 0;
+    // 24 sites: stages 3-5 read y from global (see tile_body).
+    if (L.c.N == 24 && L.stage >= 3) p.pre_bytes[0] = 0;
   }
   return p;
 }

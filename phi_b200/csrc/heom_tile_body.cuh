@@ -521,11 +521,12 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   // element e of the tile: node nd = e / E, offset w = e % E; complex128
   // buffers are indexed (n0 + nd) * E + w, X / k buffers (n0 + nd) * ES + w.
   auto preD = [&](int b) { return reinterpret_cast<const double2 *>(PreBase + pre_off[b]); };
-  // The 24-site mixed kernel reads the RKF45 state y of stages 3-5 from global
-  // memory instead of staging it (a zero-byte operand slot): 18 KB less shared
-  // memory per tile, 3 CTAs per SM instead of 2 (c5 step 1.56 -> 1.52 ms; the
-  // same change was slower for 7 sites, whose CTA count it does not raise).
-  constexpr bool kYGlobal = MIXED && N == 24;
+  // The 24-site kernels read the RKF45 state y of stages 3-5 from global
+  // memory instead of staging it (a zero-byte operand slot): 9-18 KB less
+  // shared memory per tile and one more CTA per SM (c5 step, mixed 1.56 ->
+  // 1.52 ms, FP64 3.16 -> 3.11 ms; the same change was slower for 7 sites,
+  // whose CTA count it does not raise).
+  constexpr bool kYGlobal = N == 24;
   auto preX = [&](int b) { return reinterpret_cast<const TX *>(PreBase + pre_off[b]); };
   double emax = 0.0;
   // Filtering: |y_new|^2 of element e goes to the first 8 bytes of its own
