@@ -208,6 +208,32 @@ __global__ void gamma_kernel(BicgVectors V, long long n, BicgScalars *sc, int j)
 }
 
 // r_i -= alpha u_{i+1} for i = 0..j; x += alpha u_0.
+// rho_kernel / gamma_kernel's scalar steps from per-tile partial sums of
+// <rhat, .> (the apply zeroed element 0 and summed them); one block, summed
+// in tile order (deterministic).
+__global__ void dot_finish_kernel(const double *parts, long long nparts, BicgScalars *sc, int which) {
+  if (solve_done(sc)) return;
+  double v[1] = {0.0};
+  for (long long b = threadIdx.x; b < nparts; b += kBlock) v[0] += parts[b];
+  block_sum<1>(v);
+  if (threadIdx.x != 0) return;
+  const double tot = v[0];
+  if (which == 0) {
+    if (!finite(tot)) {
+      fail(sc, kBicgNonFinite);
+    } else if (sc->rho0 == 0.0 || tot == 0.0) {
+      fail(sc, kBicgRhoZero);
+    } else {
+      sc->beta = sc->alpha * tot / sc->rho0;
+      sc->rho0 = tot;
+    }
+  } else {
+    if (!finite(tot)) fail(sc, kBicgNonFinite);
+    else if (tot == 0.0) fail(sc, kBicgGammaZero);
+    else sc->alpha = sc->rho0 / tot;
+  }
+}
+
 __global__ void r_update_kernel(BicgVectors V, long long n, const BicgScalars *sc, int j) {
   if (solve_done(sc)) return;
   const double a = sc->alpha;
@@ -437,6 +463,11 @@ cudaError_t bicg_launch_init(const BicgVectors &V, long long n, BicgScalars *sc,
 }
 cudaError_t bicg_launch_rho(const BicgVectors &V, long long n, BicgScalars *sc, int j, int grid, cudaStream_t s) {
   rho_kernel<<<grid, kBlock, 0, s>>>(V, n, sc, j);
+  return cudaGetLastError();
+}
+cudaError_t bicg_launch_dot_finish(const double *parts, long long nparts, BicgScalars *sc, int which,
+                                   cudaStream_t s) {
+  dot_finish_kernel<<<1, kBlock, 0, s>>>(parts, nparts, sc, which);
   return cudaGetLastError();
 }
 cudaError_t bicg_launch_u_update(const BicgVectors &V, long long n, const BicgScalars *sc, int j, int grid,

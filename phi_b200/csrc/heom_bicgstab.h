@@ -52,6 +52,12 @@ cudaError_t bicg_launch_u_update(const BicgVectors &V, long long n, const BicgSc
 cudaError_t bicg_launch_gamma(const BicgVectors &V, long long n, BicgScalars *sc, int j, int grid, cudaStream_t s);
 cudaError_t bicg_launch_r_update(const BicgVectors &V, long long n, const BicgScalars *sc, int j, int grid,
                                  cudaStream_t s);
+// The same two inner products when the apply that produced the vector
+// already summed <rhat, .> per tile (the tiled kernel, dot_part of a stage
+// launch): one block adds the nparts partials in order and runs the scalar
+// step of rho (which = 0) or gamma (which = 1).
+cudaError_t bicg_launch_dot_finish(const double *parts, long long nparts, BicgScalars *sc, int which,
+                                   cudaStream_t s);
 // Minimal-residual step over r_1..r_ell and the end-of-iteration control.
 cudaError_t bicg_launch_gram(const BicgVectors &V, long long n, BicgScalars *sc, int ell, int grid, cudaStream_t s);
 cudaError_t bicg_launch_mr_update(const BicgVectors &V, long long n, BicgScalars *sc, int ell, int grid,

@@ -31,6 +31,11 @@ struct StageLaunch {
   // writes the new state writes its flags to the other buffer.
   uint8_t *act[2] = {nullptr, nullptr};
   int act_par = 0;
+  // FP64 apply of the steady-state solver (tiled kernel): element (0,0) of
+  // node 0 of the output is zeroed and each tile writes its share of
+  // <dot_w, out> to dot_part[tile].
+  const double2 *dot_w = nullptr;
+  double *dot_part = nullptr;
   // Tiled kernel: stage input / output and k buffers in the context's
   // storage type (complex128, or complex64 in mixed precision), the
   // complex64 copies of the state, and the arithmetic.

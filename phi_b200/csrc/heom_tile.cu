@@ -121,6 +121,8 @@ TileParams tile_params_for(const StageLaunch &L) {
   p.act[0] = L.act[0];
   p.act[1] = L.act[1];
   p.act_par = L.act_par;
+  p.dot_w = (L.mode == kModeApply && !L.mixed) ? L.dot_w : nullptr;
+  p.dot_part = p.dot_w ? L.dot_part : nullptr;
   const bool mixed = L.mixed;
   const int xb = mixed ? 8 : 16;
   // Epilogue operands of this (mode, stage), in the order the epilogue reads them.

@@ -82,6 +82,8 @@ struct TileParams {
   Rkf45Ctl *ctl;
   uint8_t *act[2];               // filtering: active flags (see StageLaunch)
   int act_par;
+  const double2 *dot_w;          // FP64 apply: <dot_w, out> per tile (see StageLaunch)
+  double *dot_part;
   int npre;                      // epilogue operands prefetched
   const void *pre[kMaxPre];      // sources; slot 0 of RKF45 is chosen on the device
   int pre_bytes[kMaxPre];        // 16 (complex128) or 8 (complex64)
@@ -537,9 +539,37 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   };
   if (p.mode == kModeApply) {
     TX *out = static_cast<TX *>(p.out);
-    for (int e = tid; e < tile_elems; e += BT) {
-      const int nd = e / E, w = e - nd * E;
-      st_stream(out + (n0 + nd) * ES + w, Us[uix(e)]);
+    bool dot = false;
+    if constexpr (!MIXED) dot = p.dot_w != nullptr;
+    if (!dot) {
+      for (int e = tid; e < tile_elems; e += BT) {
+        const int nd = e / E, w = e - nd * E;
+        st_stream(out + (n0 + nd) * ES + w, Us[uix(e)]);
+      }
+    } else if constexpr (!MIXED) {
+      // Steady-state solve: the output's element (0,0) of node 0 is the
+      // eliminated unknown (zero), and the tile's share of <dot_w, out> (the
+      // real inner product of Hermitian states) goes to dot_part[tile] --
+      // the inner product the solver would otherwise read the vector for.
+      double dsum = 0.0;
+      for (int e = tid; e < tile_elems; e += BT) {
+        const int nd = e / E, w = e - nd * E;
+        const long long gx = (n0 + nd) * ES + w;
+        TX v = Us[uix(e)];
+        if (gx == 0) v = mk<TX>(0.0, 0.0);
+        st_stream(out + gx, v);
+        const double2 r = __ldg(p.dot_w + gx);
+        dsum = fma(r.x, v.x, fma(r.y, v.y, dsum));
+      }
+      for (int off = 16; off > 0; off >>= 1) dsum += __shfl_xor_sync(0xffffffffu, dsum, off);
+      double *wsum = reinterpret_cast<double *>(wmax);
+      if ((tid & 31) == 0) wsum[tid >> 5] = dsum;
+      __syncthreads();
+      if (tid == 0) {
+        double t = 0.0;
+        for (int w = 0; w < BT / 32; ++w) t += wsum[w];
+        p.dot_part[tile] = t;
+      }
     }
   } else if (p.mode == kModeRk4) {
     const int s = p.stage;

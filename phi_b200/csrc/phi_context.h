@@ -74,6 +74,10 @@ struct phi_ctx {
   // graph replays outer iterations for bicg_ell.
   phi::DeviceBuffer bicg_vecs;
   phi::DeviceBuffer bicg_sc;
+  // Per-tile partial sums of <rhat, A v> from the tiled FP64 apply (two
+  // arrays of bicg_tiles doubles); empty where the generic kernel applies.
+  phi::DeviceBuffer bicg_parts;
+  long long bicg_tiles = 0;
   int bicg_ell = 0;
   cudaGraphExec_t bicg_graph = nullptr;
 

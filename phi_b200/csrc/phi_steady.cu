@@ -10,6 +10,7 @@
 
 #include "../../include/phi_b200.h"
 #include "heom_bicgstab.h"
+#include "heom_tile.h"
 #include "heom_kernels.h"
 #include "phi_context.h"
 
@@ -28,8 +29,11 @@ int steady_err(phi_ctx *ctx, cudaError_t e, const char *where) {
 
 // out = L(in) over every node in FP64 (element (0,0) of node 0 is handled by
 // the BiCGSTAB kernels).
-cudaError_t apply_fp64(phi_ctx *ctx, const double2 *in, double2 *out, cudaStream_t s) {
+cudaError_t apply_fp64(phi_ctx *ctx, const double2 *in, double2 *out, cudaStream_t s,
+                       const double2 *dot_w = nullptr, double *dot_part = nullptr) {
   phi::StageLaunch L;
+  L.dot_w = dot_w;
+  L.dot_part = dot_part;
   L.c = ctx->c;
   L.mode = phi::kModeApply;
   L.grid = ctx->grid;
@@ -47,13 +51,24 @@ cudaError_t apply_fp64(phi_ctx *ctx, const double2 *in, double2 *out, cudaStream
 cudaError_t outer_iteration(phi_ctx *ctx, const phi::BicgVectors &V, long long n, phi::BicgScalars *sc, int ell,
                             int grid, cudaStream_t s) {
   cudaError_t e = cudaSuccess;
+  // With the tiled kernel the applies that produce u_{j+1} and r_{j+1} also
+  // zero their element (0,0) of node 0 and sum <rhat, .> per tile, so gamma
+  // and the next rho need only a one-block finish instead of a pass over
+  // two state-size vectors each.
+  const bool fused = ctx->bicg_parts.ptr != nullptr;
+  double *pu = fused ? ctx->bicg_parts.as<double>() : nullptr;
+  double *pr = fused ? pu + ctx->bicg_tiles : nullptr;
   for (int j = 0; j < ell && e == cudaSuccess; ++j) {
-    if (j > 0) e = phi::bicg_launch_rho(V, n, sc, j, grid, s);
+    if (j > 0) e = fused ? phi::bicg_launch_dot_finish(pr, ctx->bicg_tiles, sc, 0, s)
+                         : phi::bicg_launch_rho(V, n, sc, j, grid, s);
     if (e == cudaSuccess) e = phi::bicg_launch_u_update(V, n, sc, j, grid, s);
-    if (e == cudaSuccess) e = apply_fp64(ctx, V.u[j], V.u[j + 1], s);
-    if (e == cudaSuccess) e = phi::bicg_launch_gamma(V, n, sc, j, grid, s);
+    if (e == cudaSuccess) e = apply_fp64(ctx, V.u[j], V.u[j + 1], s, fused ? V.rhat : nullptr, pu);
+    if (e == cudaSuccess)
+      e = fused ? phi::bicg_launch_dot_finish(pu, ctx->bicg_tiles, sc, 1, s)
+                : phi::bicg_launch_gamma(V, n, sc, j, grid, s);
     if (e == cudaSuccess) e = phi::bicg_launch_r_update(V, n, sc, j, grid, s);
-    if (e == cudaSuccess) e = apply_fp64(ctx, V.r[j], V.r[j + 1], s);
+    const bool rho_next = fused && j + 1 < ell;  // the last r_{j+1} goes to the Gram step instead
+    if (e == cudaSuccess) e = apply_fp64(ctx, V.r[j], V.r[j + 1], s, rho_next ? V.rhat : nullptr, pr);
   }
   if (e == cudaSuccess) e = phi::bicg_launch_gram(V, n, sc, ell, grid, s);
   if (e == cudaSuccess) e = phi::bicg_launch_mr_update(V, n, sc, ell, grid, s);
@@ -111,6 +126,13 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     if (ctx->bicg_vecs.alloc(bytes * nvec) != cudaSuccess) {
       ctx->error = "steady_state: allocation of " + std::to_string(nvec) + " Krylov vectors (" +
                    std::to_string(bytes * nvec) + " bytes) failed";
+      return PHI_E_OOM;
+    }
+  }
+  if (phi::tile_kernel_available(ctx->c) && !ctx->bicg_parts.ptr) {
+    ctx->bicg_tiles = phi::tile_count(ctx->c, false);
+    if (ctx->bicg_tiles > 0 && ctx->bicg_parts.alloc((size_t)2 * ctx->bicg_tiles * sizeof(double)) != cudaSuccess) {
+      ctx->error = "steady_state: allocation of the per-tile partial sums failed";
       return PHI_E_OOM;
     }
   }
