@@ -6,7 +6,8 @@
 // take milliseconds.  Freed blocks are kept per (device, size) and handed to
 // the next allocation of exactly that size, as a caching allocator does.  A
 // free still synchronises the device first (the guarantee cudaFree gives),
-// so no block is reused while a kernel of its previous owner runs.  At most
+// so no block is reused while a kernel of its previous owner runs; blocks
+// are filed under the device they live on.  At most
 // kMaxCachedBytes stay cached; an allocation that fails with out-of-memory
 // releases the cache and retries; phi_gpu_release_cached_memory releases it
 // on request.  Nothing is released at process exit (the driver reclaims it).
@@ -86,8 +87,23 @@ cudaError_t cached_device_alloc(void **out, size_t bytes) {
 
 void cached_device_free(void *p, size_t bytes) {
   if (!p) return;
-  int device = 0;
-  if (cudaDeviceSynchronize() != cudaSuccess || cudaGetDevice(&device) != cudaSuccess) {
+  // The block is filed under the device it lives on (the current device may
+  // have changed since it was allocated), after that device has finished
+  // its work.
+  cudaPointerAttributes attr{};
+  int current = 0;
+  if (cudaPointerGetAttributes(&attr, p) != cudaSuccess || attr.type != cudaMemoryTypeDevice ||
+      cudaGetDevice(&current) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(p);
+    return;
+  }
+  const int device = attr.device;
+  bool synced = true;
+  if (device != current) synced = cudaSetDevice(device) == cudaSuccess;
+  synced = synced && cudaDeviceSynchronize() == cudaSuccess;
+  if (device != current) cudaSetDevice(current);
+  if (!synced) {
     cudaFree(p);
     return;
   }
