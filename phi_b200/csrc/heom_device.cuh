@@ -20,6 +20,25 @@ constexpr int kMaxTier = 250;    // L limit (multi-index stored as uint8)
 
 enum BathKind : int { kIndependent = 0, kDiagonal = 1, kFull = 2 };
 
+// Raises a kernel's dynamic shared-memory limit to `bytes` when that is above
+// the default 48 KiB.  The limit belongs to the function on each device, so
+// the largest size set so far is remembered per device ordinal in `seen`
+// (one array per kernel, owned by its launcher; ordinals past the array set
+// the attribute on every launch).
+constexpr int kSmemLimitDevices = 64;
+template <class Kernel>
+inline cudaError_t raise_smem_limit(Kernel kern, size_t bytes, int (&seen)[kSmemLimitDevices]) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const bool tracked = dev >= 0 && dev < kSmemLimitDevices;
+  if (tracked && seen[dev] >= (int)bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess && tracked) seen[dev] = (int)bytes;
+  return e;
+}
+
 // Read-only problem constants, built on the host once per context.  Mirrors
 // what PHI keeps per node (HierarchyNode prefactors, hierarchy_node.h:139-208)
 // but stores it per term: the per-node values are recomputed in registers.

@@ -515,13 +515,9 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
 template <int GROUP, int KIND>
 cudaError_t launch_group(const StageParams &p, size_t smem, int grid, cudaStream_t stream) {
   auto kern = heom_stage_kernel<GROUP, KIND>;
-  static thread_local int configured_bytes = -1;
-  if ((int)smem > 48 * 1024 && configured_bytes < (int)smem) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    if (e != cudaSuccess) return e;
-    configured_bytes = (int)smem;
-  }
+  static thread_local int configured[kSmemLimitDevices] = {};
+  cudaError_t e = raise_smem_limit(kern, smem, configured);
+  if (e != cudaSuccess) return e;
   kern<<<grid, 256, smem, stream>>>(p);
   return cudaGetLastError();
 }

@@ -40,12 +40,9 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
   const size_t smem_max = tile_smem<N, KT, MIXED, BT>(p.c.T, kMaxPre, max_bytes);
   auto kern = heom_tile_kernel<N, KT, MIXED>;
-  static thread_local int configured = -1;
-  if (smem_max > 48 * 1024 && configured < (int)smem_max) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_max);
-    if (e != cudaSuccess) return e;
-    configured = (int)smem_max;
-  }
+  static thread_local int configured[kSmemLimitDevices] = {};
+  cudaError_t e = raise_smem_limit(kern, smem_max, configured);
+  if (e != cudaSuccess) return e;
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
   kern<<<(unsigned)tiles, BT, tile_smem<N, KT, MIXED, BT>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
   return cudaGetLastError();

@@ -133,12 +133,9 @@ size_t tl_smem_bytes(int N) { return (size_t)3 * N * N * sizeof(double2); }
 
 cudaError_t launch_tl(const TlLaunch &p, cudaStream_t stream) {
   const size_t smem = tl_smem_bytes(p.c.N);
-  static thread_local int configured = -1;
-  if (smem > 48 * 1024 && configured < (int)smem) {
-    cudaError_t e = cudaFuncSetAttribute(tl_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    configured = (int)smem;
-  }
+  static thread_local int configured[kSmemLimitDevices] = {};
+  cudaError_t e = raise_smem_limit(tl_kernel, smem, configured);
+  if (e != cudaSuccess) return e;
   tl_kernel<<<p.c.nb, kTlThreads, smem, stream>>>(p);
   return cudaGetLastError();
 }
