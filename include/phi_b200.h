@@ -290,8 +290,8 @@ PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out
  * driver and gives the bytes released. */
 PHI_API int64_t phi_gpu_release_cached_memory(void);
 
-/* Copies the text of the last error on this context (or of the last failed
- * create when ctx is NULL) into buf. */
+/* Copies the text of the last error on this context (or of the calling
+ * thread's last failed create when ctx is NULL) into buf. */
 PHI_API int phi_gpu_last_error(const phi_ctx *ctx, char *buf, size_t len);
 
 /* ---- Restart files --------------------------------------------------------
@@ -314,6 +314,7 @@ PHI_API int phi_restart_read_file_ex(const char *path, int32_t num_states, int64
 PHI_API int phi_restart_write_file_ex(const char *path, int32_t num_states, int64_t num_nodes,
                                       const double *state, double time, double timestep,
                                       const double *matrices, int64_t num_matrices);
+/* Copies the text of the last failed restart call of the calling thread into buf. */
 PHI_API int phi_restart_last_error(char *buf, size_t len);
 /* The context's state and time to / from a restart file (RestartInput and
  * RestartFile of PHI's parameter file).  A time-local context writes its

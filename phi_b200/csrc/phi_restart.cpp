@@ -22,7 +22,7 @@
 
 namespace {
 
-std::string g_restart_error;
+thread_local std::string g_restart_error;  // per calling thread, as the create error is
 
 int fail(int code, const std::string &msg) {
   g_restart_error = msg;

@@ -74,3 +74,37 @@ def test_malformed_restart_files_are_rejected(tmp_path, edit):
     path.write_text(text)
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
         capi.restart_read(path, n, M)
+
+
+def test_restart_error_text_is_per_thread(tmp_path):
+    """A failed restart call on one thread leaves another thread's error text alone."""
+    import ctypes
+    import threading
+
+    lib = capi.load()
+
+    def last_error():
+        buf = ctypes.create_string_buffer(1024)
+        assert lib.phi_restart_last_error(buf, 1024) == 0
+        return buf.value.decode()
+
+    n, M = _dims(_problem())
+    missing = tmp_path / "missing.txt"
+    with pytest.raises(capi.PhiError):
+        capi.restart_read(missing, n, M)
+    mine = last_error()
+    assert mine
+    seen = {}
+
+    def other():
+        seen["before"] = last_error()
+        with pytest.raises(capi.PhiError):
+            capi.restart_read(tmp_path / "also_missing.txt", n, M)
+        seen["after"] = last_error()
+
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen["before"] == ""
+    assert "also_missing" in seen["after"] or seen["after"] != mine
+    assert last_error() == mine
