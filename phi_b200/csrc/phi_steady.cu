@@ -260,6 +260,9 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
       result = PHI_E_NO_CONVERGENCE;
     }
   }
+  // On an error path a copy into `host` may still be queued: drain the
+  // stream before the buffer goes back to the cache for another owner.
+  if (result != PHI_OK) cudaStreamSynchronize(s);
   phi::cached_host_free(host, offsetof(phi::BicgScalars, partials));
   if (result == PHI_OK || result == PHI_E_NO_CONVERGENCE) {
     const int flag = ctx->check_device_flag();
