@@ -147,9 +147,10 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_baseline_port(p, seconds_budget=12.0):
+def cpu_baseline_port(p, seconds_budget=10.0):
     """The oracle (C restatement, one core) on a bounded sample: Liouvillian
-    applies over the full hierarchy until ~seconds_budget of CPU work."""
+    applies over the full hierarchy until seconds_budget of CPU work (at most
+    400 applies)."""
     import numpy as np
     from oracle import oracle as O
     o = O.Oracle(p)
@@ -161,7 +162,7 @@ def cpu_baseline_port(p, seconds_budget=12.0):
     while True:
         o.apply(s)
         n_apply += 1
-        if time.perf_counter() - t0 > seconds_budget / 2 or n_apply >= 16:
+        if time.perf_counter() - t0 >= seconds_budget or n_apply >= 400:
             break
     dt = time.perf_counter() - t0
     return {"value": n_apply * o.M / dt, "unit": UNIT, "cores": 1, "kind": "port",
