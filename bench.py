@@ -147,6 +147,35 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def cpu_model() -> str:
+    """CPU model name of this host (from /proc/cpuinfo) and its logical CPU count."""
+    name = "unknown"
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                name = ln.split(":", 1)[1].strip()
+                break
+    except OSError:
+        pass
+    return f"{name} ({os.cpu_count()} logical CPUs)"
+
+
+def reference_fixture(workload_name):
+    """rho_0 of the reference build for the full-size RKF45 workload (the
+    committed fixture tests/golden/ref_fullsize.json), or None."""
+    import numpy as np
+    path = os.path.join(ROOT, "tests", "golden", "ref_fullsize.json")
+    if not os.path.exists(path):
+        return None
+    for c in json.load(open(path))["cases"]:
+        if c["id"] == f"{workload_name}/rkf45" and c.get("rho0_colmajor"):
+            v = np.array(c["rho0_colmajor"])
+            n = int(round(len(v) ** 0.5))
+            rho = (v[:, 0] + 1j * v[:, 1]).reshape(n, n).T
+            return rho, c
+    return None
+
+
 def cpu_baseline_port(p, seconds_budget=10.0):
     """The oracle (C restatement, one core) on a bounded sample: Liouvillian
     applies over the full hierarchy until seconds_budget of CPU work (at most
@@ -165,7 +194,7 @@ def cpu_baseline_port(p, seconds_budget=10.0):
         if time.perf_counter() - t0 >= seconds_budget or n_apply >= 400:
             break
     dt = time.perf_counter() - t0
-    return {"value": n_apply * o.M / dt, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": n_apply * o.M / dt, "unit": UNIT, "cores": 1, "kind": "port", "cpu": cpu_model(),
             "sample": f"{n_apply} Liouvillian applies over the {o.M}-node hierarchy "
                       f"({dt:.1f} s, single-thread C restatement)"}
 
@@ -231,6 +260,7 @@ def run_reference_arm(args):
     res.update({"value": value, "ms_per_step": per_step * 1e3,
                 "rkf45_steps_per_s": 1.0 / per_step,
                 "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                                 "cpu": cpu_model(),
                                  "sample": f"{steps} RKF45 steps to t = {t_end:.4g} ps in {secs:.0f} s by PHI's "
                                            f"own integration timer, {threads} threads"},
                 "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
@@ -240,18 +270,19 @@ def run_reference_arm(args):
 def run_steps(h, steps, fresh):
     """Exactly `steps` attempted RKF45 steps of the 1 ps propagation; when a
     propagation reaches t_end it restarts from rho(0) on the device
-    (phi_gpu_reset).  Returns (steps, propagations finished)."""
-    done = finished = 0
+    (phi_gpu_reset).  Returns (steps, propagations finished, advance calls)."""
+    done = finished = calls = 0
     dt0 = DT0 if fresh else -1.0
     while done < steps:
         st = h.rkf45_advance(dt0, T_END, TOL, MIN_DT, steps - done)
+        calls += 1
         done += int(st["steps"])
         dt0 = -1.0
         if st["final_time"] >= T_END:
             h.reset(0.0)
             finished += 1
             dt0 = DT0
-    return done, finished
+    return done, finished, calls
 
 
 def batch_step_bytes(problems, mixed):
@@ -480,7 +511,7 @@ def main():
     ev1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
-    steps_done, propagations = run_steps(h, args.steps, False)
+    steps_done, propagations, advance_calls = run_steps(h, args.steps, False)
     ev1.record(stream)
     ev1.synchronize()
     torch.cuda.synchronize()
@@ -552,7 +583,7 @@ def main():
     torch.cuda.synchronize()
     e0o, e1o = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0o.record(so)
-    other_steps, _ = run_steps(ho, args.steps, False)
+    other_steps, _, _ = run_steps(ho, args.steps, False)
     e1o.record(so)
     e1o.synchronize()
     other_ms_per_step = e0o.elapsed_time(e1o) / max(other_steps, 1)
@@ -564,6 +595,15 @@ def main():
         rho_full[pr] = (hf.rho0(), stf)
         hf.close()
     rho_err = float(np.abs(rho_full[capi.PHI_PREC_MIXED][0] - rho_full[capi.PHI_PREC_FP64][0]).max())
+    # Against the reference build's own FP64 rho_0 of the same full run.
+    vs_ref = None
+    fx = reference_fixture(WORKLOAD)
+    if fx is not None:
+        rho_ref, meta = fx
+        vs_ref = {"fp64": float(np.abs(rho_full[capi.PHI_PREC_FP64][0] - rho_ref).max()),
+                  "mixed": float(np.abs(rho_full[capi.PHI_PREC_MIXED][0] - rho_ref).max()),
+                  "reference_steps": meta["steps"], "reference_accepted": meta["accepted_steps"],
+                  "source": "tests/golden/ref_fullsize.json (reference build, %.17g)"}
 
     if rank == 0:
         peak, peak_kind = peaks()
@@ -596,10 +636,13 @@ def main():
                              f"{9 * M * E * 16 / 1e6:.0f} MB > 126 MB L2"},
             "rkf45_steps_per_s": total_steps / (t_max / 1e3),
             "rho0_err_vs_fp64": rho_err,
-            "meets_1e-6": rho_err <= 1e-6,
+            "rho0_err_vs_reference": vs_ref,
+            "meets_1e-6": rho_err <= 1e-6 and (vs_ref is None or vs_ref["mixed"] <= 1e-6),
             "full_run": {"t_end_ps": T_END,
                          "fp64_steps": int(rho_full[capi.PHI_PREC_FP64][1]["steps"]),
-                         "mixed_steps": int(rho_full[capi.PHI_PREC_MIXED][1]["steps"])},
+                         "fp64_accepted": int(rho_full[capi.PHI_PREC_FP64][1]["accepted"]),
+                         "mixed_steps": int(rho_full[capi.PHI_PREC_MIXED][1]["steps"]),
+                         "mixed_accepted": int(rho_full[capi.PHI_PREC_MIXED][1]["accepted"])},
             "other_precision": {"precision": "fp64" if other == capi.PHI_PREC_FP64 else "mixed",
                                 "ms_per_step": other_ms_per_step,
                                 "value": 6 * M / (other_ms_per_step / 1e3)},
@@ -617,7 +660,9 @@ def main():
                     "d2h_bytes_per_step": d2h / max(e2e_steps, 1),
                     "what": "create (hierarchy built on device) + full 1 ps RKF45 + rho_0 read-back + "
                             "destroy, host wall clock through the C ABI (second of two runs)", "rho0_trace": float(np.trace(rho0).real)},
-            "gpu_launches": ((steps_done + 15) // 16) * 16 * 7,
+            # six stage kernels + the control kernel per attempted step, and the
+            # complex64 copy of y each advance call starts with (mixed)
+            "gpu_launches": 7 * steps_done + (advance_calls if prec == capi.PHI_PREC_MIXED else 0),
             "clocks": clocks,
         }
         if WORKLOAD == "ring24":

@@ -281,9 +281,32 @@ PHI_API int phi_gpu_set_time(phi_ctx *ctx, double time);
  * two stage-input buffers live in a built-in 16 MiB device array, so the
  * state may be at most 8 MiB (PHI_E_INVALID above that); all calls share
  * that array, so calls that overlap on the GPU race.  The first call on a
- * device looks up the array's address; make it before any stream capture. */
+ * device looks up the array's address; make it before any stream capture
+ * (after cudaDeviceReset on that device, reload the library).  Like one
+ * phi_gpu_rk4 step, each call advances the context's time-local truncation
+ * matrices by dt and makes the step's new filter flags current; the
+ * context's time and its own state are unchanged.  d_out is therefore one
+ * step after d_in when d_in continues the trajectory those matrices and
+ * flags belong to (phi_gpu_set_state resets both).  The call does not
+ * synchronise: a bounded device wait that gave up inside it is reported by
+ * phi_gpu_check_device_flag or by the next synchronising call. */
 PHI_API int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_out, double dt,
                                      void *stream);
+
+/* Waits for the work queued on `stream` (the context's own stream when NULL)
+ * and reports whether a bounded device wait of the context's kernels gave up
+ * since the last check (PHI_E_TIMEOUT; the flag is then cleared).  For
+ * callers of the non-synchronising entry points (phi_gpu_apply_device,
+ * phi_gpu_rk4_step_noalloc).  No counterpart in the reference. */
+PHI_API int phi_gpu_check_device_flag(phi_ctx *ctx, void *stream);
+
+/* Test hook for the timeout path: the poll limit of the tiled stage kernels'
+ * first wait on a tile's bulk copies (0 restores the built-in limit, a
+ * negative value gives up at once).  A kernel that gives up sets the
+ * context's device flag, waits with the built-in limit for its own copies
+ * and returns; the next checking call reports PHI_E_TIMEOUT and the context
+ * stays usable.  No counterpart in the reference. */
+PHI_API int phi_gpu_debug_set_wait_limit(phi_ctx *ctx, int64_t polls);
 
 /* Device memory of destroyed contexts is kept (up to 8 GiB) for the next
  * allocation of the same size in this process; this returns it to the

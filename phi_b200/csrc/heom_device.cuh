@@ -71,6 +71,10 @@ struct HeomConsts {
   const uint8_t *pair_i;     // N(N+1)/2 upper-triangle pairs (i <= j)
   const uint8_t *pair_j;
   int *err_flag;             // set by a kernel whose bounded wait gave up
+  // Poll limit of the tile kernels' first wait on a tile's bulk copy: 0 the
+  // built-in limit, < 0 give up at once (a test of the timeout path; the
+  // drain of the CTA's own copies keeps the built-in limit).
+  long long first_wait_polls;
   // Adaptive hierarchy filtering (PHI's FilterTolerance, independent baths):
   // a node whose largest |element| drops below filter_tol stops feeding its
   // neighbours until it rises above it again.

@@ -118,8 +118,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 }
 // Bounded wait for the phase with the given parity of `bar` to complete;
 // false if it gave up.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-  for (long long i = 0; i < kMaxPolls; ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  long long polls = kMaxPolls) {
+  for (long long i = 0; i < polls; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -378,10 +379,14 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
     for (int t = 0; t < T; ++t) d += nts[tid * T + t] * __ldg(c.nu + t);
     deph[tid] = d;
   }
-  bool ok = mbar_wait_bounded(&bars[0], par0);
+  const long long polls0 = c.first_wait_polls == 0 ? kMaxPolls : (c.first_wait_polls < 0 ? 0 : c.first_wait_polls);
+  bool ok = mbar_wait_bounded(&bars[0], par0, polls0);
   __syncthreads();  // deph visible
   if (!__syncthreads_and(ok)) {
     if (tid == 0) atomicOr(c.err_flag, 1);
+    // Drain this tile's own copies with the built-in limit, so no copy is
+    // still writing into shared memory when the CTA stops.
+    mbar_wait_bounded(&bars[0], par0);
     if (p.npre > 0) mbar_wait_bounded(&bars[1], par1);
     return -1;
   }

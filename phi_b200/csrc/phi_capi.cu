@@ -610,17 +610,24 @@ extern "C" int phi_gpu_get_rho0(const phi_ctx *cctx, double *rho0) {
   return PHI_OK;
 }
 
-int phi_ctx::check_device_flag() {
+int phi_ctx::check_device_flag() { return check_device_flag_on(stream); }
+
+int phi_ctx::check_device_flag_on(cudaStream_t s) {
   int flag = 0;
-  cudaError_t e = cudaMemcpyAsync(&flag, cbuf.err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+  cudaError_t e = cudaMemcpyAsync(&flag, cbuf.err_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(this, e, "device flag read");
   if (flag) {
-    cudaMemsetAsync(cbuf.err_flag.ptr, 0, sizeof(int), stream);
+    cudaMemsetAsync(cbuf.err_flag.ptr, 0, sizeof(int), s);
     error = "a device wait on a bulk copy gave up (bounded mbarrier wait)";
     return PHI_E_TIMEOUT;
   }
   return PHI_OK;
+}
+
+extern "C" int phi_gpu_check_device_flag(phi_ctx *ctx, void *stream) {
+  if (!ctx) return PHI_E_INVALID;
+  return ctx->check_device_flag_on(stream ? static_cast<cudaStream_t>(stream) : ctx->stream);
 }
 
 extern "C" int phi_gpu_apply_device(phi_ctx *ctx, const void *d_in, void *d_out, void *stream) {
@@ -686,6 +693,13 @@ extern "C" int phi_gpu_reset(phi_ctx *ctx, double time) {
   PHI_CUDA(ctx, ctx->reset_annealing());
   ctx->time = time;
   ctx->rkf45_started = false;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_debug_set_wait_limit(phi_ctx *ctx, int64_t polls) {
+  if (!ctx) return PHI_E_INVALID;
+  ctx->c.first_wait_polls = polls;
+  ctx->release_graphs();  // captured launches carry the old constants
   return PHI_OK;
 }
 

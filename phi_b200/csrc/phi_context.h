@@ -104,6 +104,7 @@ struct phi_ctx {
   void release_graphs();
   // PHI_E_TIMEOUT if a kernel's bounded wait gave up since the last check.
   int check_device_flag();
+  int check_device_flag_on(cudaStream_t s);  // after the work queued on s
   // Marks every node active (a newly set state), enqueued on `stream`.
   cudaError_t reset_filter();
   // Points a stage launch at the flag buffers (no-op when filtering is off).

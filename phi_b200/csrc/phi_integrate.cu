@@ -342,17 +342,28 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
   if (!ctx->host_ctl) PHI_CK(phi::cached_host_alloc(&ctx->host_ctl, sizeof(phi::Rkf45Ctl)));
   phi::Rkf45Ctl *hpin = static_cast<phi::Rkf45Ctl *>(ctx->host_ctl);
   int result = PHI_OK;
-  // Two graphs in flight: the done flag of launch j is read while launch j+1
-  // runs; steps after completion are no-ops on the device.
-  long long launched = 0;
-  PHI_CK(cudaGraphLaunch(ctx->rkf45_graph, ctx->stream));
-  launched += kGraphSteps;
+  // Exactly max_steps attempted steps are enqueued: whole graphs of
+  // kGraphSteps, then the remainder as direct launches.  Two chunks are in
+  // flight: the done flag after chunk j is read while chunk j+1 runs; steps
+  // after completion are no-ops on the device.
+  long long launched = 0, graphs = 0;
+  auto enqueue_chunk = [&]() -> cudaError_t {
+    const long long left = hc.max_steps - launched;
+    if (left >= kGraphSteps) {
+      launched += kGraphSteps;
+      ++graphs;
+      return cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
+    }
+    for (; launched < hc.max_steps; ++launched) {
+      cudaError_t e = enqueue_rkf45_step(ctx, ctx->stream);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+  };
+  PHI_CK(enqueue_chunk());
   for (;;) {
     cudaError_t e = cudaSuccess;
-    if (launched < hc.max_steps) {
-      e = cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
-      launched += kGraphSteps;
-    }
+    if (launched < hc.max_steps) e = enqueue_chunk();
     if (e == cudaSuccess) e = cudaMemcpyAsync(hpin, ctx->ctl.ptr, sizeof(phi::Rkf45Ctl), cudaMemcpyDeviceToHost, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) {
@@ -360,8 +371,13 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
       break;
     }
     if (hpin->done) break;
+    if (launched >= hc.max_steps) {  // every step ran and the device did not stop
+      ctx->error = "rkf45: the device control block did not finish after max_steps steps";
+      result = PHI_E_CUDA;
+      break;
+    }
   }
-  ctx->graph_launches += launched / kGraphSteps;
+  ctx->graph_launches += graphs;
   if (result == PHI_OK) {
     hc = *hpin;
     if (hc.ycur == 1) {

@@ -21,7 +21,17 @@
 //    nothing needs clearing between calls;
 //  * the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  The address is kept for the life of the
+//    library: after cudaDeviceReset on that device, reload the library;
+//  * the step reads and advances the context's own step-dependent state as
+//    one phi_gpu_rk4 step would: time-local truncation matrices (two half
+//    steps of dt/2) and filter flags (the new flags become the current ones).
+//    The context's time and its own state buffer do not change.  So d_out is
+//    one step after d_in only when d_in continues the trajectory those
+//    matrices and flags belong to (phi_gpu_set_state resets both);
+//  * the call does not synchronise, so a bounded device wait that gave up
+//    inside it is reported by the next call that checks the context's device
+//    flag (phi_gpu_check_device_flag, or any synchronising entry point).
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -87,10 +97,11 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
                  "-byte limit of the built-in scratch; use phi_gpu_rk4";
     return PHI_E_INVALID;
   }
-  int prev_device = 0;
+  int prev_device = -1;
   cudaError_t e = cudaGetDevice(&prev_device);
   const int device = ctx->desc.device;
-  if (e == cudaSuccess && prev_device != device) e = cudaSetDevice(device);
+  const bool restore = e == cudaSuccess && prev_device != device;
+  if (restore) e = cudaSetDevice(device);
   void *scratch = nullptr;
   if (e == cudaSuccess) e = scratch_address(device, &scratch);
   if (e == cudaSuccess) {
@@ -132,7 +143,7 @@ extern "C" int phi_gpu_rk4_step_noalloc(phi_ctx *ctx, const void *d_in, void *d_
       e = cudaMemcpyAsync(ctx->active[0].ptr, ctx->active[1].ptr, (size_t)ctx->hier.M,
                           cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
   }
-  if (prev_device != device) cudaSetDevice(prev_device);
+  if (restore) cudaSetDevice(prev_device);
   if (e != cudaSuccess) {
     ctx->error = std::string("rk4_step_noalloc: ") + cudaGetErrorString(e);
     return PHI_E_CUDA;

@@ -394,10 +394,67 @@ def make_restart_tl_fixture():
     print("time-local restart fixture written", flush=True)
 
 
+# Benchmarked configurations at their full size, run by the reference build
+# with all host threads (its results do not depend on the thread count):
+# (case id, configs builder, builder kwargs, method, timestep, t_end).
+FULLSIZE_CASES = [
+    ("frenkel7_L6/rkf45", "frenkel7", {}, "rkf45", 0.001, 1.0),
+    ("frenkel7_L6/rk4", "frenkel7", {}, "rk4", 0.001, 0.3),
+    ("ring24_L4/rkf45", "ring24", {}, "rkf45", 0.001, 0.5),
+    ("chain4_L8/rk4", "chain4", {}, "rk4", 0.001, 0.1),
+]
+
+
+def make_fullsize_fixture(only=None):
+    """ref_fullsize.json: rho_0 (%.17g) and PHI's own step counts for the
+    benchmarked configurations at full size (38,760 / 20,475 / 125,970
+    nodes).  Each case runs the reference for minutes; the file is
+    rewritten after every case so a partial run keeps what it finished."""
+    path = os.path.join(HERE, "ref_fullsize.json")
+    done = {}
+    if os.path.exists(path):
+        done = {c["id"]: c for c in json.load(open(path))["cases"]}
+    threads = os.cpu_count() or 1
+    for cid, builder, kw, method, dt, t_end in FULLSIZE_CASES:
+        if only and cid not in only:
+            continue
+        p = getattr(configs, builder)(**kw)
+        with tempfile.TemporaryDirectory() as d:
+            prm, out, rho_f = (os.path.join(d, x) for x in ("in.prm", "out.txt", "rho.txt"))
+            with open(prm, "w") as f:
+                f.write(O.param_file_text(p, timestep=dt, t_end=t_end, output_min_step=t_end,
+                                          output_file=out).replace("verbose=-2", "verbose=0"))
+            subprocess.run([O.REF_DRIVER, "run", prm, method, str(threads), rho_f], check=True,
+                           timeout=3600, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            rho = O.parse_rho_file(rho_f, p.num_states)
+            secs = float(open(rho_f).read().split("\n")[0].split()[1])
+            steps = accepted = None
+            for ln in open(out):
+                if ln.startswith("#Total number of integration steps"):
+                    steps = int(ln.split("=")[1])
+                if ln.startswith("#Total number of accepted integration steps"):
+                    accepted = int(ln.split("=")[1])
+        done[cid] = {"id": cid, "builder": builder, "kwargs": kw, "seed": int(p.seed), "method": method,
+                     "timestep": dt, "t_end": t_end, "rkf45_tolerance": float(p.rkf45_tolerance),
+                     "rkf45_mindt": float(p.rkf45_minimum_timestep), "steps": steps,
+                     "accepted_steps": accepted, "threads": threads, "launch_seconds": secs,
+                     "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]}
+        with open(path, "w") as f:
+            json.dump({"generator": "tests/golden/make_golden.py fullsize",
+                       "cases": [done[c[0]] for c in FULLSIZE_CASES if c[0] in done]}, f, indent=0)
+        print(f"{cid}: {steps} steps ({accepted} accepted), {secs:.1f} s", flush=True)
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PHI_REFERENCE_ROOT")
+    if not ref_root:
+        raise SystemExit("usage: make_golden.py <reference source root> [fixture]  "
+                         "(or set PHI_REFERENCE_ROOT)")
     if not O.ref_available():
-        raise SystemExit("build the reference first: make -C oracle")
+        raise SystemExit("build the reference first: make -C oracle REF_SRC=<reference>/src")
+    if len(sys.argv) > 2 and sys.argv[2] == "fullsize":
+        make_fullsize_fixture(sys.argv[3:] or None)
+        return
     if len(sys.argv) > 2 and sys.argv[2] == "restart":
         make_restart_fixture()
         return

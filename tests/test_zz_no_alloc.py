@@ -59,6 +59,48 @@ def test_noalloc_step_matches_allocating_rk4(make):
     assert np.abs(got2 - ref2).max() <= FP64_TOL * scale
 
 
+def _time_local():
+    p = cases.random_problem("independent", n=3, matsubara=2, truncation=3, seed=2)
+    p.use_time_local_truncation = True
+    return p
+
+
+def _filtered():
+    p = cases.random_problem("independent", n=3, matsubara=2, truncation=5, seed=2)
+    p.filter_tolerance = 1e-3
+    return p
+
+
+@pytest.mark.parametrize("make", [_time_local, _filtered], ids=["time_local_n3", "filtered_n3"])
+def test_noalloc_steps_carry_context_matrices_and_flags(make):
+    """A time-local or filtered context: each call advances the context's
+    truncation matrices and filter flags like one phi_gpu_rk4 step, so two
+    calls from set_state(s0) equal two allocating steps from s0."""
+    p = make()
+    with Hierarchy(p) as h:
+        s0 = h.get_state()
+        s0 = s0 + 1e-4 * cases.random_hermitian_state(h.num_nodes, p.num_states, seed=7)
+        h.set_state(s0)
+        h.time = 0.0
+        h.rk4(DT, 2 * DT)
+        ref, act_ref, q_ref = h.get_state(), h.active(), h.time_local()
+        h.set_state(s0)  # matrices and flags back to their start
+        h.time = 0.0
+        a = torch.tensor(s0, dtype=torch.float64, device="cuda")
+        b, c = torch.empty_like(a), torch.empty_like(a)
+        _noalloc_step(h, a, b)
+        _noalloc_step(h, b, c)
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        assert h.lib.phi_gpu_check_device_flag(h.ctx, stream) == capi.PHI_OK
+        torch.cuda.synchronize()
+        got, act, q = c.cpu().numpy(), h.active(), h.time_local()
+    if p.filter_tolerance > 0:
+        assert np.array_equal(act, act_ref) and 0 < int(act.sum()) < len(act)
+    if p.use_time_local_truncation:
+        assert np.abs(q - q_ref).max() <= 1e-14 * np.abs(q_ref).max()
+    assert np.abs(got - ref).max() <= FP64_TOL * np.abs(ref).max()
+
+
 def test_noalloc_rejects_states_beyond_its_scratch():
     p = configs.frenkel7()  # 38,760 nodes: 30.4 MB of state > 8 MiB
     with Hierarchy(p) as h:
