@@ -308,6 +308,21 @@ PHI_API int phi_gpu_check_device_flag(phi_ctx *ctx, void *stream);
  * stays usable.  No counterpart in the reference. */
 PHI_API int phi_gpu_debug_set_wait_limit(phi_ctx *ctx, int64_t polls);
 
+/* Test hooks for RKF45 parity.  An accept decision compares a computed
+ * error estimate with the tolerance, so two FP64 evaluations that differ by
+ * rounding can decide a borderline attempt differently and then follow
+ * different step sequences.  set_rkf45_replay makes the next phi_gpu_rkf45
+ * runs take the given decisions for their first `count` attempts (0 reject,
+ * 1 accept, 2 accept and grow the step by the grow factor; the last-step
+ * clamp still applies) and record the error estimate of their first
+ * `trace_capacity` attempts; count = trace_capacity = 0 switches both off.
+ * get_rkf45_errors copies the recorded estimates of the last run.  No
+ * counterpart in the reference (its accept test is Rkf45Integrate's,
+ * hierarchy_integrator.cc:2355). */
+PHI_API int phi_gpu_debug_set_rkf45_replay(phi_ctx *ctx, const int8_t *decisions, int64_t count,
+                                           int64_t trace_capacity);
+PHI_API int phi_gpu_debug_get_rkf45_errors(phi_ctx *ctx, double *out, int64_t capacity, int64_t *count);
+
 /* Device memory of destroyed contexts is kept (up to 8 GiB) for the next
  * allocation of the same size in this process; this returns it to the
  * driver and gives the bytes released. */

@@ -13,6 +13,7 @@
 #include <complex.h>
 #include <float.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -667,9 +668,53 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
   }
 }
 
+/* Threads of the node loop (1 unless oracle_set_threads raised it).  Only
+ * independent-bath hierarchies are split: each node's derivative depends on
+ * read-only inputs alone, so the result does not depend on the split (PHI's
+ * own results are thread-count independent, too).  The diagonal and full
+ * updaters keep one thread: FullBath carries its work matrix from node to
+ * node, as PHI's per-thread scratch does. */
+static int g_threads = 1;
+
+void oracle_set_threads(int n) { g_threads = n > 0 ? n : 1; }
+
+typedef struct {
+  const oracle_ctx *c;
+  const cplx *rho;
+  cplx *out;
+  int64_t begin, end;
+} apply_range;
+
+static void *apply_range_run(void *arg) {
+  apply_range *r = (apply_range *)arg;
+  cplx *t = (cplx *)calloc((size_t)(r->c->N * r->c->N), sizeof(cplx));
+  for (int64_t i = r->begin; i < r->end; ++i) apply_node(r->c, i, r->rho, r->out, t);
+  free(t);
+  return NULL;
+}
+
 static void apply_all(const oracle_ctx *c, const cplx *rho, cplx *out, cplx *temp) {
   /* FullBath's work matrix starts zeroed, as new Complex[] does (:100-102). */
   for (int k = 0; k < c->N * c->N; ++k) temp[k] = 0;
+  if (g_threads > 1 && c->kind == ORACLE_BATH_INDEPENDENT && c->M >= 4 * g_threads) {
+    pthread_t th[64];
+    apply_range rg[64];
+    const int nt = g_threads < 64 ? g_threads : 64;
+    for (int t = 0; t < nt; ++t) {
+      rg[t].c = c;
+      rg[t].rho = rho;
+      rg[t].out = out;
+      rg[t].begin = c->M * t / nt;
+      rg[t].end = c->M * (t + 1) / nt;
+    }
+    int started = 0;
+    for (int t = 1; t < nt; ++t, ++started)
+      if (pthread_create(&th[t], NULL, apply_range_run, &rg[t]) != 0) break;
+    apply_range_run(&rg[0]);
+    for (int t = 1; t <= started; ++t) pthread_join(th[t], NULL);
+    for (int t = started + 1; t < nt; ++t) apply_range_run(&rg[t]);  /* threads that did not start */
+    return;
+  }
   for (int64_t i = 0; i < c->M; ++i) apply_node(c, i, rho, out, temp);
 }
 
@@ -846,6 +891,13 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start
 int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double start_time,
                      double end_time, double tolerance, double min_dt,
                      int64_t *accepted_out, double *final_time, double *final_dt) {
+  return oracle_rkf45_trace(c, state_d, dt0, start_time, end_time, tolerance, min_dt, accepted_out,
+                            final_time, final_dt, NULL, 0);
+}
+
+int64_t oracle_rkf45_trace(const oracle_ctx *c, double *state_d, double dt0, double start_time,
+                           double end_time, double tolerance, double min_dt, int64_t *accepted_out,
+                           double *final_time, double *final_dt, double *err_trace, int64_t trace_cap) {
   /* Rkf45Integrate, hierarchy_integrator.cc:1797-2573.  The step-size
    * bookkeeping mirrors the reference: every tableau coefficient is scaled by
    * dt once and then multiplied in place by the grow/shrink factor, and the
@@ -920,6 +972,9 @@ int64_t oracle_rkf45(const oracle_ctx *c, double *state_d, double dt0, double st
       const double diff = cabs(y4 - x[j]);
       max_diff = (diff > max_diff) ? diff : max_diff;
     }
+    /* The error estimate of every attempt, for callers that check the
+     * accept decisions (test infrastructure). */
+    if (err_trace && i < trace_cap) err_trace[i] = max_diff;
     /* Accept test (:2355) taken on the step size of this attempt. */
     if (max_diff < tolerance || mydt * creal(dtdn) < min_dt) {
       memcpy(y, x, sizeof(cplx) * (size_t)total);

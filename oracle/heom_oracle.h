@@ -121,6 +121,16 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state, double dt, double start_t
 int64_t oracle_rkf45(const oracle_ctx *c, double *state, double dt0, double start_time,
                      double end_time, double tolerance, double min_dt,
                      int64_t *accepted, double *final_time, double *final_dt);
+/* Threads of the Liouvillian's node loop for independent baths (default 1;
+ * results do not depend on it). */
+void oracle_set_threads(int n);
+
+/* oracle_rkf45 that also records the max-abs error estimate of every
+ * attempted step (the value PHI's accept test compares, :2355) in
+ * err_trace[0 .. trace_cap-1]. */
+int64_t oracle_rkf45_trace(const oracle_ctx *c, double *state, double dt0, double start_time,
+                           double end_time, double tolerance, double min_dt, int64_t *accepted,
+                           double *final_time, double *final_dt, double *err_trace, int64_t trace_cap);
 
 #ifdef __cplusplus
 }

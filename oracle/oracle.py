@@ -79,6 +79,12 @@ def load():
     lib.oracle_rkf45.restype = c_int64
     lib.oracle_rkf45.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
                                  c_double, POINTER(c_int64), POINTER(c_double), POINTER(c_double)]
+    lib.oracle_set_threads.restype = None
+    lib.oracle_set_threads.argtypes = [ctypes.c_int]
+    lib.oracle_rkf45_trace.restype = c_int64
+    lib.oracle_rkf45_trace.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
+                                       c_double, POINTER(c_int64), POINTER(c_double), POINTER(c_double),
+                                       c_void_p, c_int64]
     _lib = lib
     return lib
 
@@ -260,19 +266,24 @@ class Oracle:
         rows = [_from_colmajor(traj[r * E2:(r + 1) * E2], self.n) for r in range(k)]
         return s, int(steps), times[:k].copy(), np.array(rows)
 
-    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0, continue_run=False):
+    def rkf45(self, state, dt0, t_end, tol, min_dt, start_time=0.0, continue_run=False, trace_capacity=0):
         """RKF45 from `state`; run state (flags, time-local matrices) as
-        for rk4."""
+        for rk4.  With trace_capacity > 0 the result also holds `errors`, the
+        error estimate of every attempted step."""
         if not continue_run:
             self.reset_run_state()
         s = np.ascontiguousarray(state, np.float64).copy()
         acc = c_int64()
         tf = c_double()
         dtf = c_double()
-        steps = self.lib.oracle_rkf45(self.ctx, s.ctypes.data, dt0, start_time, t_end, tol, min_dt,
-                                      ctypes.byref(acc), ctypes.byref(tf), ctypes.byref(dtf))
-        return s, {"steps": int(steps), "accepted": acc.value, "final_time": tf.value,
-                   "final_dt": dtf.value}
+        trace = np.zeros(trace_capacity, np.float64)
+        steps = self.lib.oracle_rkf45_trace(self.ctx, s.ctypes.data, dt0, start_time, t_end, tol, min_dt,
+                                            ctypes.byref(acc), ctypes.byref(tf), ctypes.byref(dtf),
+                                            trace.ctypes.data if trace_capacity else None, trace_capacity)
+        st = {"steps": int(steps), "accepted": acc.value, "final_time": tf.value, "final_dt": dtf.value}
+        if trace_capacity:
+            st["errors"] = trace[:min(int(steps), trace_capacity)].copy()
+        return s, st
 
     def rho0(self, state):
         return _from_colmajor(np.asarray(state)[:2 * self.n * self.n], self.n)
@@ -401,6 +412,11 @@ def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_to
     if getattr(p, "use_time_local_truncation", False):
         lines.append("TimeLocal=1")
     return "\n".join(lines) + "\n"
+
+
+def set_threads(n: int) -> None:
+    """Threads of the oracle's independent-bath Liouvillian (default 1)."""
+    load().oracle_set_threads(int(n))
 
 
 def ref_available() -> bool:

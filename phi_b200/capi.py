@@ -142,6 +142,8 @@ SIGNATURES = [
     ("phi_gpu_rk4_step_noalloc", c_int, [c_void_p, c_void_p, c_void_p, c_double, c_void_p]),
     ("phi_gpu_check_device_flag", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_debug_set_wait_limit", c_int, [c_void_p, c_int64]),
+    ("phi_gpu_debug_set_rkf45_replay", c_int, [c_void_p, c_void_p, c_int64, c_int64]),
+    ("phi_gpu_debug_get_rkf45_errors", c_int, [c_void_p, c_void_p, c_int64, POINTER(c_int64)]),
     ("phi_gpu_last_error", c_int, [c_void_p, c_char_p, c_size_t]),
     ("phi_restart_read_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, POINTER(c_double), POINTER(c_double)]),
     ("phi_restart_write_file", c_int, [c_char_p, c_int32, c_int64, c_void_p, c_double, c_double]),

@@ -114,6 +114,14 @@ struct Rkf45Ctl {
   int tl_pending;
   double a[5];
   double tl_h_accept;
+  // Test hooks (null / 0 in normal runs): decisions to take instead of the
+  // error test for the first forced_len attempts of a run (0 reject, 1
+  // accept, 2 accept and grow the step), and the error estimate of each of
+  // the first trace_cap attempts.
+  const signed char *forced;
+  long long forced_len;
+  double *err_trace;
+  long long trace_cap;
 };
 
 // RK4 device bookkeeping (only the rho_0 trajectory needs it).

@@ -474,6 +474,8 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
   ctl->tl_pending = 0;
   const double err = __longlong_as_double((long long)ctl->err_bits);
   ctl->err_bits = 0ull;
+  const long long attempt = ctl->steps;
+  if (ctl->err_trace && attempt < ctl->trace_cap) ctl->err_trace[attempt] = err;
   ctl->steps += 1;
   if (!(err == err) || err > 1.0e300) {
     ctl->nonfinite = 1;
@@ -481,7 +483,13 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
     ctl->status = 2;
     return;
   }
-  if (err < ctl->tol || ctl->dt * ctl->dtdn < ctl->min_dt) {
+  bool accept = err < ctl->tol || ctl->dt * ctl->dtdn < ctl->min_dt;
+  bool grow = err < ctl->tol / 10;
+  if (ctl->forced && attempt < ctl->forced_len) {
+    accept = ctl->forced[attempt] != 0;
+    grow = ctl->forced[attempt] == 2;
+  }
+  if (accept) {
     // Time-local matrices advance by the rest of this attempt (dt - a5).
     ctl->tl_h_accept = ctl->dt - ctl->a[4];
     ctl->tl_pending = 1;
@@ -489,7 +497,7 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
     ctl->time += ctl->dt;
     ctl->accepted += 1;
     if (err > ctl->max_error) ctl->max_error = err;
-    bool update = err < ctl->tol / 10;
+    bool update = grow;
     if (ctl->time + ctl->dt > ctl->end_time) {
       update = true;
       ctl->dtup = (ctl->end_time - ctl->time) / ctl->dt;

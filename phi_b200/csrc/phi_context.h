@@ -81,6 +81,11 @@ struct phi_ctx {
   int bicg_ell = 0;
   cudaGraphExec_t bicg_graph = nullptr;
 
+  // RKF45 test hooks: forced accept decisions and the per-attempt error
+  // trace (phi_gpu_debug_set_rkf45_replay).
+  phi::DeviceBuffer rkf45_forced, rkf45_trace;
+  long long rkf45_forced_len = 0, rkf45_trace_cap = 0;
+
   // RKF45 state kept between calls (phi_gpu_rkf45_advance with dt0 <= 0).
   phi::Rkf45Ctl rkf45_last{};
   bool rkf45_started = false;

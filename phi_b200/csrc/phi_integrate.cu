@@ -326,6 +326,10 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
   hc.done = ctx->time < t_end ? 0 : 1;
   hc.status = 0;
   hc.nonfinite = 0;
+  hc.forced = ctx->rkf45_forced_len ? ctx->rkf45_forced.as<signed char>() : nullptr;
+  hc.forced_len = ctx->rkf45_forced_len;
+  hc.err_trace = ctx->rkf45_trace_cap ? ctx->rkf45_trace.as<double>() : nullptr;
+  hc.trace_cap = ctx->rkf45_trace_cap;
   PHI_CK(cudaMemcpyAsync(ctx->ctl.ptr, &hc, sizeof(hc), cudaMemcpyHostToDevice, ctx->stream));
   if (ctx->mixed())  // stage-0 input of the first step: complex64 copy of y (ycur = 0)
     PHI_CK(phi::launch_to_c64(ctx->y.as<double2>(), ctx->y32.as<float2>(), ctx->hier.M,
@@ -424,6 +428,41 @@ extern "C" int phi_gpu_rkf45_advance(phi_ctx *ctx, double dt0, double t_end, dou
     return PHI_E_INVALID;
   }
   return run_rkf45(ctx, dt0, t_end, tol, min_dt, steps, false, stats);
+}
+
+extern "C" int phi_gpu_debug_set_rkf45_replay(phi_ctx *ctx, const int8_t *decisions, int64_t count,
+                                              int64_t trace_capacity) {
+  if (!ctx || count < 0 || trace_capacity < 0 || (count > 0 && !decisions)) return PHI_E_INVALID;
+  for (int64_t i = 0; i < count; ++i)
+    if (decisions[i] < 0 || decisions[i] > 2) {
+      ctx->error = "rkf45 replay: decisions are 0 (reject), 1 (accept) or 2 (accept and grow)";
+      return PHI_E_INVALID;
+    }
+  ctx->rkf45_forced_len = 0;
+  ctx->rkf45_trace_cap = 0;
+  if (count > 0) {
+    if (ctx->rkf45_forced.bytes < (size_t)count) {
+      ctx->rkf45_forced.reset();
+      PHI_CK(ctx->rkf45_forced.alloc((size_t)count));
+    }
+    PHI_CK(cudaMemcpy(ctx->rkf45_forced.ptr, decisions, (size_t)count, cudaMemcpyHostToDevice));
+  }
+  if (trace_capacity > 0 && ctx->rkf45_trace.bytes < (size_t)trace_capacity * sizeof(double)) {
+    ctx->rkf45_trace.reset();
+    PHI_CK(ctx->rkf45_trace.alloc((size_t)trace_capacity * sizeof(double)));
+  }
+  ctx->rkf45_forced_len = count;
+  ctx->rkf45_trace_cap = trace_capacity;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_debug_get_rkf45_errors(phi_ctx *ctx, double *out, int64_t capacity, int64_t *count) {
+  if (!ctx || !count || (capacity > 0 && !out)) return PHI_E_INVALID;
+  const long long n = std::min<long long>(ctx->rkf45_last.steps, ctx->rkf45_trace_cap);
+  *count = n;
+  const long long m = std::min<long long>(n, capacity);
+  if (m > 0) PHI_CK(cudaMemcpy(out, ctx->rkf45_trace.ptr, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost));
+  return PHI_OK;
 }
 
 extern "C" int phi_gpu_stream(const phi_ctx *ctx, void **stream) {
