@@ -282,9 +282,12 @@ int build_hierarchy_device(int T, int L, DeviceHierarchy *out, std::string *err,
   DeviceBuffer d_tab, d_first_q, d_keep, d_bsum, d_total, d_tfirst, d_bad;
   cudaError_t e = cudaSuccess;
   auto chk = [&](cudaError_t x) { if (x != cudaSuccess && e == cudaSuccess) e = x; };
-  chk(out->mi.alloc((size_t)M * T));
-  chk(out->next.alloc((size_t)M * T * sizeof(int32_t)));
-  chk(out->prev.alloc((size_t)M * T * sizeof(int32_t)));
+  // 64 bytes past the end of each table: the tiled kernels bulk-copy a
+  // tile's records as a 16-byte aligned window, which may reach up to 15
+  // bytes past the last record.
+  chk(out->mi.alloc((size_t)M * T + 64));
+  chk(out->next.alloc((size_t)M * T * sizeof(int32_t) + 64));
+  chk(out->prev.alloc((size_t)M * T * sizeof(int32_t) + 64));
   chk(out->rank_to_id.alloc((size_t)M * sizeof(int32_t)));
   chk(d_tab.alloc(tab.size() * sizeof(unsigned long long)));
   chk(d_tfirst.alloc((size_t)(L + 2) * sizeof(long long)));

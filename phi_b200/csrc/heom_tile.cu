@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "heom_tile_body.cuh"
@@ -24,6 +25,16 @@ struct TileBlock {
   static constexpr int threads = (MIXED && N == 24) ? 320 : kTileThreads;
 };
 
+// Experiment switch during development: PHI_TILE_PIPELINE=0 selects the
+// one-tile-per-CTA kernel.
+bool tile_pipeline_enabled() {
+  static const bool on = [] {
+    const char *v = std::getenv("PHI_TILE_PIPELINE");
+    return !(v && v[0] == '0');
+  }();
+  return on;
+}
+
 template <int N, int KT, bool MIXED>
 __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
                                   TileMinBlocks<KT, MIXED, TileBlock<N, MIXED>::threads>::value)
@@ -33,17 +44,298 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
   tile_body<N, KT, MIXED, TileBlock<N, MIXED>::threads>(p, blockIdx.x, smem_raw, 0u, 0u);
 }
 
+// ---- persistent pipelined kernel ----
+//
+// A CTA stays resident and walks the tiles blockIdx.x, blockIdx.x +
+// gridDim.x, ...  While tile i computes, the stage input X and the neighbour
+// records (next / prev ids and occupations, contiguous per tile) of tile i+1
+// arrive in the other of two shared-memory slots by cp.async.bulk; the
+// epilogue operands of tile i (y, accumulator, k_r) are issued when tile i
+// starts and land while its pair loop runs.  H, the Matsubara factors, the
+// pair list, c_t, the dephasing rates and the prefactor tables are staged
+// once per CTA.  Three mbarriers: one per slot (phase parity (i >> 1) & 1 for
+// the CTA's i-th tile) and one for the epilogue operands (parity i & 1).
+template <int N, int KT, bool MIXED, int BT>
+struct PipeLayout {
+  using S = TileShape<N, MIXED, KT, BT>;
+  static constexpr int T = N * KT;
+  static constexpr int ES = MIXED ? S::EP : S::E;
+  static constexpr int XB = MIXED ? 8 : 16;
+  static constexpr int RB = MIXED ? 4 : 8;  // bytes of the arithmetic type
+  static constexpr size_t r16(size_t b) { return (b + 15) / 16 * 16; }
+  static constexpr size_t r128(size_t b) { return (b + 127) / 128 * 128; }
+  // One slot: the tile's X, then its next ids, prev ids (int32) and
+  // occupations (uint8), each copied from the 16-byte aligned window around
+  // the tile's records (up to 3 ids / 15 bytes of slack on either side).
+  static constexpr size_t kSlotX = r128((size_t)S::NT * ES * XB);
+  static constexpr size_t kSlotIds = r16(((size_t)S::NT * T + 8) * 4);
+  static constexpr size_t kSlotMi = r16((size_t)S::NT * T + 32);
+  static constexpr size_t kSlot = r128(kSlotX + 2 * kSlotIds + kSlotMi);
+  static constexpr size_t kSlots = 128;                       // after the 3 mbarriers
+  static constexpr size_t kUs = kSlots + 2 * kSlot;           // derivative tile
+  static constexpr size_t kPre = kUs + r128((size_t)S::NT * S::EU * XB);
+};
+
+template <int N, int KT, bool MIXED, int BT>
+size_t pipe_smem(int T, int L, int npre, const int *pre_bytes) {
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = PipeLayout<N, KT, MIXED, BT>;
+  size_t b = Lay::kPre;
+  for (int i = 0; i < npre; ++i)
+    b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
+  const int W = L + 2;
+  b += (size_t)S::E * Lay::XB;                                        // H
+  b += (size_t)(S::NT + 24 + BT / 32 + T) * sizeof(double);           // deph, coef, warp maxima, rates
+  b += (size_t)(2 * S::NT * T + 2 * T + S::E + 2 * T * W) * Lay::RB;  // cn, cp, c_t, mats, prefactor tables
+  b += (size_t)(S::NT * 3 * T) * sizeof(int);                         // ids, occupations
+  b += 2 * S::P + 16;
+  return b;
+}
+
+template <int N, int KT, bool MIXED>
+__global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
+                                  TileMinBlocks<KT, MIXED, TileBlock<N, MIXED>::threads>::value)
+    heom_tile_pipe_kernel(TileParams p) {
+  constexpr int BT = TileBlock<N, MIXED>::threads;
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = PipeLayout<N, KT, MIXED, BT>;
+  using TX = typename TileArith<MIXED>::TX;
+  using R = typename TileArith<MIXED>::R;
+  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES, T = N * KT;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const HeomConsts &c = p.c;
+  const int tid = threadIdx.x;
+  if (p.mode == kModeRkf45 && *(volatile int *)&p.ctl->done) return;  // uniform across the grid
+
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kUs);
+  unsigned char *PreBase = smem_raw + Lay::kPre;
+  uint32_t pre_off[kMaxPre];
+  size_t tail = Lay::kPre;
+  {
+    uint32_t acc_off = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      pre_off[b] = acc_off;
+      if (b < p.npre) acc_off += ((uint32_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
+    }
+    tail += acc_off;
+  }
+  const int W = c.L + 2;
+  TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                           // E
+  double *deph = reinterpret_cast<double *>(Hs + E);                          // NT
+  double *coef = deph + NT;                                                   // 24
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // BT / 32
+  double *rate = reinterpret_cast<double *>(wmax + BT / 32);                  // T
+  R *cn = reinterpret_cast<R *>(rate + T);                                    // NT*T
+  R *cp = cn + NT * T;                                                        // NT*T
+  R *ccr = cp + NT * T;                                                       // 2T
+  R *mats = ccr + 2 * T;                                                      // E
+  R *sqn = mats + E;                                                          // T*W
+  R *sqp = sqn + T * W;                                                       // T*W
+  int *ids = reinterpret_cast<int *>(sqp + T * W);                            // NT*2T
+  int *nts = ids + NT * 2 * T;                                                // NT*T
+  unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
+  unsigned char *pj = pi + P;
+
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_init(&bars[2], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  int ycur = 0;
+  if (p.mode == kModeRkf45) {
+    ycur = p.ctl->ycur;
+    if (tid < 24) coef[tid] = p.ctl->coef[tid];
+  }
+  const bool hreal = c.h_real;
+  R *Hr = reinterpret_cast<R *>(Hs);
+  if (hreal) {
+    for (int i = tid; i < E; i += BT) Hr[i] = (R)__ldg(c.H + i).x;
+  } else {
+    for (int i = tid; i < E; i += BT) Hs[i] = from_d2<TX>(__ldg(c.H + i));
+  }
+  for (int i = tid; i < E; i += BT) mats[i] = (R)__ldg(c.mats_elem + i);
+  for (int i = tid; i < P; i += BT) {
+    pi[i] = __ldg(c.pair_i + i);
+    pj[i] = __ldg(c.pair_j + i);
+  }
+  for (int t = tid; t < T; t += BT) {
+    const double2 ct = __ldg(c.corr + t);
+    ccr[2 * t] = (R)ct.x;
+    ccr[2 * t + 1] = (R)ct.y;
+    rate[t] = __ldg(c.nu + t);
+  }
+  for (int q = tid; q < T * W; q += BT) {
+    sqn[q] = (R)__ldg(c.sq_next + q);
+    sqp[q] = (R)__ldg(c.sq_prev + q);
+  }
+  __syncthreads();  // barriers initialised, constants visible
+
+  const long long ntiles = (c.M + NT - 1) / NT;
+  const TX *xin;
+  if (p.mode == kModeRkf45 && p.stage == 0)
+    xin = MIXED ? static_cast<const TX *>(p.y32buf[ycur]) : reinterpret_cast<const TX *>(p.ybuf[ycur]);
+  else
+    xin = static_cast<const TX *>(p.x);
+  // Filtering: an inactive neighbour contributes nothing (the DoNext /
+  // DoPrevious overrides of IndependentBathAdaptiveTruncation,
+  // hierarchy_updater.cc:256-303).
+  const uint8_t *act_in = c.filtered ? p.act[p.mode == kModeRkf45 ? ycur : p.act_par] : nullptr;
+  const long long polls0 = c.first_wait_polls == 0 ? kMaxPolls : (c.first_wait_polls < 0 ? 0 : c.first_wait_polls);
+
+  // Thread 0: the X and neighbour records of `tile` into slot s.
+  auto issue_slot = [&](long long tile, int s) {
+    const long long n0 = tile * NT;
+    const int nt = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
+    unsigned char *b = smem_raw + Lay::kSlots + (size_t)s * Lay::kSlot;
+    const long long q0 = n0 * T, q1 = q0 + (long long)nt * T;
+    const long long a4 = q0 & ~3ll, e4 = (q1 + 3) & ~3ll, a16 = q0 & ~15ll, e16 = (q1 + 15) & ~15ll;
+    const uint32_t xbytes = (uint32_t)(nt * ES * Lay::XB), idbytes = (uint32_t)((e4 - a4) * 4),
+                   mibytes = (uint32_t)(e16 - a16);
+    mbar_expect_tx(&bars[s], xbytes + 2 * idbytes + mibytes);
+    bulk_g2s(b, xin + n0 * ES, xbytes, &bars[s]);
+    bulk_g2s(b + Lay::kSlotX, c.next + a4, idbytes, &bars[s]);
+    bulk_g2s(b + Lay::kSlotX + Lay::kSlotIds, c.prev + a4, idbytes, &bars[s]);
+    bulk_g2s(b + Lay::kSlotX + 2 * Lay::kSlotIds, c.mi + a16, mibytes, &bars[s]);
+  };
+  // Thread 0: the epilogue operands of `tile`.
+  auto issue_pre = [&](long long tile) {
+    const long long n0 = tile * NT;
+    const int nt = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
+    uint32_t pbytes = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b)
+      if (b < p.npre) pbytes += (uint32_t)(nt * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
+    mbar_expect_tx(&bars[2], pbytes);
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      if (b >= p.npre) break;
+      if (p.pre_bytes[b] == 0) continue;  // read from global in the epilogue
+      const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
+      if (b == 0 && p.mode == kModeRkf45)
+        src = static_cast<const unsigned char *>(p.pre_bytes[0] == 8 ? p.y32buf[ycur] : (const void *)p.ybuf[ycur]);
+      const int stride = p.pre_bytes[b] == 16 ? E : ES;
+      bulk_g2s(PreBase + pre_off[b], src + (size_t)n0 * stride * p.pre_bytes[b],
+               (uint32_t)(nt * stride * p.pre_bytes[b]), &bars[2]);
+    }
+  };
+
+  long long tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) issue_slot(tile, 0);
+  double emax = 0.0;
+  int i = 0;
+  bool failed = false, next_issued = false;
+  for (; tile < ntiles; ++i, tile += gridDim.x) {
+    const int s = i & 1;
+    const long long n0 = tile * NT;
+    const int nt_here = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
+    next_issued = tile + gridDim.x < ntiles;
+    if (tid == 0) {
+      if (next_issued) issue_slot(tile + gridDim.x, s ^ 1);
+      if (p.npre > 0) issue_pre(tile);
+    }
+    if (!__syncthreads_and(mbar_wait_bounded(&bars[s], (uint32_t)(i >> 1) & 1u, polls0))) {
+      failed = true;
+      break;
+    }
+    // Per (node, term): neighbour element offsets (-1 when absent or
+    // inactive), occupation and the prefactor magnitudes for it; per node:
+    // the dephasing rate.
+    const unsigned char *sb = smem_raw + Lay::kSlots + (size_t)s * Lay::kSlot;
+    const TX *Xs = reinterpret_cast<const TX *>(sb);
+    const int q0 = (int)((n0 * T) & 15);
+    const int *nx_s = reinterpret_cast<const int *>(sb + Lay::kSlotX) + (q0 & 3);
+    const int *pv_s = reinterpret_cast<const int *>(sb + Lay::kSlotX + Lay::kSlotIds) + (q0 & 3);
+    const uint8_t *mi_s = sb + Lay::kSlotX + 2 * Lay::kSlotIds + q0;
+    for (int q = tid; q < nt_here * T; q += BT) {
+      const int nd = q / T, t = q - nd * T;
+      const int nx = nx_s[q], pv = pv_s[q], nt = mi_s[q];
+      const bool nx_on = nx >= 0 && (!act_in || __ldg(act_in + nx));
+      const bool pv_on = pv >= 0 && (!act_in || __ldg(act_in + pv));
+      ids[nd * 2 * T + t] = nx_on ? nx * ES : -1;
+      ids[nd * 2 * T + T + t] = pv_on ? pv * ES : -1;
+      nts[q] = nt;
+      cn[q] = sqn[t * W + nt];
+      cp[q] = sqp[t * W + nt];
+    }
+    if (tid < nt_here) {
+      double d = 0.0;
+      for (int t = 0; t < T; ++t) d += mi_s[tid * T + t] * rate[t];
+      deph[tid] = d;
+    }
+    __syncthreads();
+    tile_pairs<N, KT, MIXED, BT>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
+    if (!__syncthreads_and(p.npre == 0 || mbar_wait_bounded(&bars[2], (uint32_t)i & 1u))) {
+      failed = true;
+      break;
+    }
+    tile_epilogue<N, KT, MIXED, BT>(p, Xs, Us, PreBase, pre_off, coef, wmax, tile, n0, nt_here, ycur, emax);
+    tile_flags<N, KT, MIXED, BT>(p, Us, n0, nt_here, ycur);
+    __syncthreads();  // slot s, the operands, Us and the per-tile arrays are reused
+  }
+  if (failed) {
+    // Record the failure and drain this CTA's copies in flight with the
+    // built-in limit, so none is still writing into shared memory at exit.
+    if (tid == 0) atomicOr(c.err_flag, 1);
+    const int s = i & 1;
+    mbar_wait_bounded(&bars[s], (uint32_t)(i >> 1) & 1u);
+    if (next_issued) mbar_wait_bounded(&bars[s ^ 1], (uint32_t)((i + 1) >> 1) & 1u);
+    if (p.npre > 0) mbar_wait_bounded(&bars[2], (uint32_t)i & 1u);
+    return;
+  }
+  if (p.mode == kModeRkf45 && p.stage == 5) tile_error_max<MIXED, BT>(p, emax, wmax);
+}
+
+// Resident CTAs per SM of a kernel at a dynamic shared-memory size and the
+// SM count of the current device, cached per (kernel, size, device).
+struct OccEntry {
+  const void *fn;
+  size_t smem;
+  int dev;
+  int grid;
+};
+
+int persistent_grid(const void *fn, int threads, size_t smem) {
+  static thread_local OccEntry cache[64];
+  static thread_local int used = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  for (int k = 0; k < used; ++k)
+    if (cache[k].fn == fn && cache[k].smem == smem && cache[k].dev == dev) return cache[k].grid;
+  int sms = 0, blocks = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, fn, threads, smem) != cudaSuccess) return 0;
+  const int grid = sms * (blocks > 0 ? blocks : 1);
+  if (used < 64) cache[used++] = OccEntry{fn, smem, dev, grid};
+  return grid;
+}
+
 template <int N, int KT, bool MIXED>
 cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
   constexpr int BT = TileBlock<N, MIXED>::threads;
   using S = TileShape<N, MIXED, KT, BT>;
+  const long long tiles = (p.c.M + S::NT - 1) / S::NT;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
+  if (tile_pipeline_enabled()) {
+    const size_t smem_max = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, kMaxPre, max_bytes);
+    auto kern = heom_tile_pipe_kernel<N, KT, MIXED>;
+    static thread_local int configured[kSmemLimitDevices] = {};
+    cudaError_t e = raise_smem_limit(kern, smem_max, configured);
+    if (e != cudaSuccess) return e;
+    const size_t smem = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, p.npre, p.pre_bytes);
+    const int cap = persistent_grid((const void *)kern, BT, smem);
+    if (cap <= 0) return cudaErrorInvalidConfiguration;
+    const long long grid = tiles < cap ? tiles : cap;
+    kern<<<(unsigned)grid, BT, smem, stream>>>(p);
+    return cudaGetLastError();
+  }
   const size_t smem_max = tile_smem<N, KT, MIXED, BT>(p.c.T, kMaxPre, max_bytes);
   auto kern = heom_tile_kernel<N, KT, MIXED>;
   static thread_local int configured[kSmemLimitDevices] = {};
   cudaError_t e = raise_smem_limit(kern, smem_max, configured);
   if (e != cudaSuccess) return e;
-  const long long tiles = (p.c.M + S::NT - 1) / S::NT;
   kern<<<(unsigned)tiles, BT, tile_smem<N, KT, MIXED, BT>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
   return cudaGetLastError();
 }
@@ -142,7 +434,7 @@ TileParams tile_params_for(const StageLaunch &L) {
     }
   } else if (L.mode == kModeRkf45) {
     if (L.stage == 0) {
-      p.npre = mixed ? 1 : 0;  // y (chosen on the device)
+      p.npre = 0;              // y (or y32) is the stage input itself
     } else if (L.stage <= 4) {
       p.npre = 1 + L.stage;    // y, k_0 .. k_{s-1}
       for (int r = 0; r < L.stage; ++r) {
@@ -157,8 +449,11 @@ TileParams tile_params_for(const StageLaunch &L) {
         p.pre_bytes[1 + r] = xb;
       }
     }
-    // 24 sites: stages 3-5 read y from global (see tile_body).
-    if (L.c.N == 24 && L.stage >= 3) p.pre_bytes[0] = 0;
+    // Slot 0 (y, chosen on the device): complex64 y32 for the mixed stage
+    // inputs of stages 1-4; read from global memory in mixed stage 5 and in
+    // the 24-site FP64 stages 3-5 (see tile_epilogue).
+    if (mixed && L.stage >= 1 && L.stage <= 4) p.pre_bytes[0] = 8;
+    if ((mixed && L.stage == 5) || (!mixed && L.c.N == 24 && L.stage >= 3)) p.pre_bytes[0] = 0;
   }
   return p;
 }

@@ -231,167 +231,37 @@ static __device__ __noinline__ void tile_filter_flags(const unsigned char *us, i
   }
 }
 
-// KT = terms per site (K + 1) under PHI's identity site map.
-// One tile (NT consecutive nodes of one hierarchy) of one stage.  The caller
-// has initialised the two mbarriers at the start of shared memory and passes
-// the phase parity each is at.  Returns 1 when the tile was skipped before
-// any copy was issued (RKF45 run finished), 0 when both barriers completed a
-// phase (barrier 1 with 0 bytes when p.npre == 0), -1 after a bounded wait gave up
-// (err_flag set; the caller must stop).
-template <int N, int KT, bool MIXED, int BT = kTileThreads>
-__device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
-                                         uint32_t par0, uint32_t par1) {
-  using S = TileShape<N, MIXED, KT, BT>;
-  using Lay = TileLayout<N, MIXED, KT, BT>;
+template <bool MIXED>
+struct TileArith {
   using TX = typename std::conditional<MIXED, float2, double2>::type;
   using R = typename std::conditional<MIXED, float, double>::type;
-  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES, NP = S::NP, EU = S::EU;
-  // tile element e (node e / E, column-major offset e % E) in the padded
-  // derivative tile
-  auto uix = [](int e) {
-    if (NP == N) return e;
-    const int nd = e / E, w = e - nd * E, c = w / N;
-    return nd * EU + (w - c * N) + c * NP;
-  };
-  const HeomConsts &c = p.c;
-  constexpr int T = N * KT;  // PHI's identity site map: K+1 terms per site
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Lay::kBars);
-  TX *Xs = reinterpret_cast<TX *>(smem_raw + Lay::kX);   // NT*ES
-  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*EU (column stride NP)
-  unsigned char *PreBase = smem_raw + Lay::kPre;
-  // Byte offsets of the prefetched epilogue operands.  Every loop over them
-  // is unrolled so the offsets stay in registers.
-  uint32_t pre_off[kMaxPre];
-  size_t tail = Lay::kPre;
-  {
-    uint32_t acc_off = 0;
-#pragma unroll
-    for (int b = 0; b < kMaxPre; ++b) {
-      pre_off[b] = acc_off;
-      if (b < p.npre) acc_off += ((uint32_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
-    }
-    tail += acc_off;
-  }
-  TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
-  double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
-  double *coef = deph + NT;                                         // 24
-  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
-  R *cn = reinterpret_cast<R *>(wmax + (BT / 32));                          // NT*T |next prefactor|
-  R *cp = cn + NT * T;                                              // NT*T prev scale
-  R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
-  R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element
-  int *ids = reinterpret_cast<int *>(mats + E);                     // NT*2T element offsets
-  int *nts = ids + NT * 2 * T;                                      // NT*T
-  unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
-  unsigned char *pj = pi + P;
+};
 
+// ---- the parts of one tile shared by the kernels ----
+// Phase 2: the derivative of every (node, upper-triangle pair) of a tile into
+// the derivative tile Us, from shared memory (the tile's stage input Xs, H,
+// per-element Matsubara factors, pair lists, per-(node, term) neighbour
+// offsets and prefactor magnitudes, dephasing rates) and, for the neighbour
+// terms, from the stage input in HBM (xin).
+template <int N, int KT, bool MIXED, int BT>
+__device__ __forceinline__ void tile_pairs(const HeomConsts &c, const typename TileArith<MIXED>::TX *Xs,
+                                           typename TileArith<MIXED>::TX *Us,
+                                           const typename TileArith<MIXED>::TX *Hs,
+                                           const typename TileArith<MIXED>::R *mats, const unsigned char *pi,
+                                           const unsigned char *pj, const int *ids,
+                                           const typename TileArith<MIXED>::R *cn,
+                                           const typename TileArith<MIXED>::R *cp,
+                                           const typename TileArith<MIXED>::R *ccr, const double *deph,
+                                           const int *nts, const typename TileArith<MIXED>::TX *xin, int nt_here) {
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = TileLayout<N, MIXED, KT, BT>;
+  using TX = typename TileArith<MIXED>::TX;
+  using R = typename TileArith<MIXED>::R;
+  constexpr int P = S::P, ES = Lay::ES, NP = S::NP, EU = S::EU;
+  constexpr int T = N * KT;
   const int tid = threadIdx.x;
-  int ycur = 0;
-  if (p.mode == kModeRkf45) {
-    if (*(volatile int *)&p.ctl->done) return 1;  // uniform across the grid
-    ycur = p.ctl->ycur;
-    if (tid < 24) coef[tid] = p.ctl->coef[tid];
-  }
-  const long long n0 = tile * NT;
-  if (n0 >= c.M) return 1;
-  // Filtering: the flags of the current state are p.act[ap], ap = ycur
-  // (RKF45) or p.act_par; the launch that writes the new state (RK4 stage 3,
-  // RKF45 stage 5 -- the candidate, kept on accept) writes its flags to
-  // p.act[ap ^ 1].  Both are recomputed from the parameters where used, so
-  // nothing of it stays live across the tile.
-  auto flag_stage = [&]() {
-    return c.filtered && ((p.mode == kModeRk4 && p.stage == 3) || (p.mode == kModeRkf45 && p.stage == 5));
-  };
-  auto act_idx = [&]() { return p.mode == kModeRkf45 ? ycur : p.act_par; };
-  const int nt_here = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
-  const TX *xin;
-  if (p.mode == kModeRkf45 && p.stage == 0)
-    xin = MIXED ? static_cast<const TX *>(p.y32buf[ycur]) : reinterpret_cast<const TX *>(p.ybuf[ycur]);
-  else
-    xin = static_cast<const TX *>(p.x);
-  const int tile_elems = nt_here * E;
-
-  // ---- t = 0: bulk prefetch of the tile's contiguous ranges ----
-  if (tid == 0) {
-    const uint32_t xbytes = (uint32_t)(nt_here * ES * Lay::XB);
-    mbar_expect_tx(&bars[0], xbytes);
-    bulk_g2s(Xs, xin + n0 * ES, xbytes, &bars[0]);
-    uint32_t pbytes = 0;
-#pragma unroll
-    for (int b = 0; b < kMaxPre; ++b)
-      if (b < p.npre) pbytes += (uint32_t)(nt_here * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
-    // Arrives on barrier 1 in every tile (with 0 bytes when nothing is
-    // prefetched), so its phase advances once per tile like barrier 0's.
-    mbar_expect_tx(&bars[1], pbytes);
-#pragma unroll
-    for (int b = 0; b < kMaxPre; ++b) {
-      if (b >= p.npre) break;
-      if (p.pre_bytes[b] == 0) continue;  // read from global in the epilogue
-      const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
-      if (b == 0 && p.mode == kModeRkf45) src = reinterpret_cast<const unsigned char *>(p.ybuf[ycur]);
-      const int stride = p.pre_bytes[b] == 16 ? E : ES;
-      const uint32_t bytes = (uint32_t)(nt_here * stride * p.pre_bytes[b]);
-      bulk_g2s(PreBase + pre_off[b], src + (size_t)n0 * stride * p.pre_bytes[b], bytes, &bars[1]);
-    }
-  }
-  // A real Hamiltonian (every in-scope workload) is kept as E reals in the
-  // same buffer, halving the products of A = H X.
   const bool hreal = c.h_real;
-  R *Hr = reinterpret_cast<R *>(Hs);
-  if (hreal) {
-    for (int i = tid; i < E; i += BT) Hr[i] = (R)__ldg(c.H + i).x;
-  } else {
-    for (int i = tid; i < E; i += BT) Hs[i] = from_d2<TX>(__ldg(c.H + i));
-  }
-  for (int i = tid; i < E; i += BT) mats[i] = (R)__ldg(c.mats_elem + i);
-  for (int i = tid; i < P; i += BT) {
-    pi[i] = __ldg(c.pair_i + i);
-    pj[i] = __ldg(c.pair_j + i);
-  }
-  const int W = c.L + 2;
-  const int tile_terms = nt_here * T;
-  // Per (node, term): neighbour ids scaled to element offsets of the stage
-  // input (-1 when absent), occupation, and the prefactor magnitudes for that
-  // occupation, so the pair loop reads shared memory only.
-  const uint8_t *act_in = c.filtered ? p.act[act_idx()] : nullptr;
-  for (int q = tid; q < tile_terms; q += BT) {
-    const int nd = q / T, t = q - nd * T;
-    const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
-    const int nt = __ldg(c.mi + n0 * T + q);
-    // An inactive neighbour contributes nothing (the DoNext / DoPrevious
-    // overrides of IndependentBathAdaptiveTruncation, hierarchy_updater.cc:256-303).
-    const bool nx_on = nx >= 0 && (!act_in || __ldg(act_in + nx));
-    const bool pv_on = pv >= 0 && (!act_in || __ldg(act_in + pv));
-    ids[nd * 2 * T + t] = nx_on ? nx * ES : -1;
-    ids[nd * 2 * T + T + t] = pv_on ? pv * ES : -1;
-    nts[q] = nt;
-    cn[q] = (R)__ldg(c.sq_next + t * W + nt);
-    cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
-  }
-  for (int t = tid; t < T; t += BT) {
-    const double2 ct = __ldg(c.corr + t);
-    ccr[2 * t] = (R)ct.x;
-    ccr[2 * t + 1] = (R)ct.y;
-  }
-  __syncthreads();  // barrier init and metadata visible
-  if (tid < nt_here) {
-    double d = 0.0;
-    for (int t = 0; t < T; ++t) d += nts[tid * T + t] * __ldg(c.nu + t);
-    deph[tid] = d;
-  }
-  const long long polls0 = c.first_wait_polls == 0 ? kMaxPolls : (c.first_wait_polls < 0 ? 0 : c.first_wait_polls);
-  bool ok = mbar_wait_bounded(&bars[0], par0, polls0);
-  __syncthreads();  // deph visible
-  if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicOr(c.err_flag, 1);
-    // Drain this tile's own copies with the built-in limit, so no copy is
-    // still writing into shared memory when the CTA stops.
-    mbar_wait_bounded(&bars[0], par0);
-    if (p.npre > 0) mbar_wait_bounded(&bars[1], par1);
-    return -1;
-  }
-
-  // ---- phase 2: derivative of every (node, pair) ----
+  const R *Hr = reinterpret_cast<const R *>(Hs);
   const R ih = (R)c.inv_hbar;
   const int items = nt_here * P;
   for (int it = tid; it < items; it += BT) {
@@ -518,24 +388,43 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       Us[nd * EU + j + i * NP] = b;
     }
   }
-  ok = p.npre == 0 || mbar_wait_bounded(&bars[1], par1);
-  if (!__syncthreads_and(ok)) {
-    if (tid == 0) atomicOr(c.err_flag, 1);
-    return -1;
-  }
+}
 
-  // ---- phase 3: epilogue over the tile's elements ----
+// Phase 3: the epilogue over a tile's elements (plain store, RK4 or RKF45
+// stage combine) from the derivative tile Us and the prefetched operands at
+// PreBase + pre_off[b]; the RKF45 stage-5 error of this thread's elements is
+// folded into emax (max of |y4 - y5|, or of its square in mixed precision).
+template <int N, int KT, bool MIXED, int BT>
+__device__ __forceinline__ void tile_epilogue(const TileParams &p, const typename TileArith<MIXED>::TX *Xs,
+                                              typename TileArith<MIXED>::TX *Us, const unsigned char *PreBase,
+                                              const uint32_t (&pre_off)[kMaxPre], const double *coef,
+                                              unsigned long long *wmax, long long tile, long long n0, int nt_here,
+                                              int ycur, double &emax) {
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = TileLayout<N, MIXED, KT, BT>;
+  using TX = typename TileArith<MIXED>::TX;
+  constexpr int E = S::E, ES = Lay::ES, NP = S::NP, EU = S::EU;
+  const HeomConsts &c = p.c;
+  const int tid = threadIdx.x;
+  const int tile_elems = nt_here * E;
+  auto uix = [](int e) {
+    if (NP == N) return e;
+    const int nd = e / E, w = e - nd * E, cc = w / N;
+    return nd * EU + (w - cc * N) + cc * NP;
+  };
+  auto flag_stage = [&]() {
+    return c.filtered && ((p.mode == kModeRk4 && p.stage == 3) || (p.mode == kModeRkf45 && p.stage == 5));
+  };
   // element e of the tile: node nd = e / E, offset w = e % E; complex128
   // buffers are indexed (n0 + nd) * E + w, X / k buffers (n0 + nd) * ES + w.
   auto preD = [&](int b) { return reinterpret_cast<const double2 *>(PreBase + pre_off[b]); };
-  // The 24-site kernels read the RKF45 state y of stages 3-5 from global
-  // memory instead of staging it (a zero-byte operand slot): 9-18 KB less
-  // shared memory per tile and one more CTA per SM (c5 step, mixed 1.56 ->
-  // 1.52 ms, FP64 3.16 -> 3.11 ms; the same change was slower for 7 sites,
-  // whose CTA count it does not raise).
-  constexpr bool kYGlobal = N == 24;
+  // RKF45 operand slot 0 is the state y: 16 bytes -> y staged in complex128;
+  // 8 bytes (mixed stages 1-4) -> its complex64 copy y32, which is all the
+  // complex64 stage input X_{s+1} = y + sum b k needs; 0 bytes -> y read from
+  // global memory in the epilogue (mixed stage 5, and the 24-site FP64
+  // kernels' stages 3-5: less shared memory per tile, more CTAs per SM).
+  const int ybytes = p.npre > 0 ? p.pre_bytes[0] : 16;
   auto preX = [&](int b) { return reinterpret_cast<const TX *>(PreBase + pre_off[b]); };
-  double emax = 0.0;
   // Filtering: |y_new|^2 of element e goes to the first 8 bytes of its own
   // slot Us[uix(e)], which only this thread reads, and only before; the
   // per-node maxima are taken from there after the loop.
@@ -620,9 +509,10 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const TX kx = Us[uix(e)];
       const double2 kv = to_d2(kx);
-      if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; FP64 stage 0: y is the input
-        const double2 ys = (s == 0 && !MIXED) ? to_d2(Xs[nd * ES + w])
-                           : ((kYGlobal && p.pre_bytes[0] == 0) ? __ldg(p.ybuf[ycur] + gd) : preD(0)[e]);
+      if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; stage 0: y is the input
+        const double2 ys = s == 0 ? to_d2(Xs[nd * ES + w])
+                           : (ybytes == 0 ? __ldg(p.ybuf[ycur] + gd)
+                                          : (ybytes == 8 ? to_d2(preX(0)[nd * ES + w]) : preD(0)[e]));
         st_stream(static_cast<TX *>(p.k[s]) + gx, kx);
         const int row = s * (s + 1) / 2;
         double2 xv = ys;
@@ -632,7 +522,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         xv = cfma(xv, kv, cf[row + s]);
         out[gx] = from_d2<TX>(xv);
       } else {      // pre = {y, k0, k2, k3, k4}
-        const double2 ys = (kYGlobal && p.pre_bytes[0] == 0) ? __ldg(p.ybuf[ycur] + gd) : preD(0)[e];
+        const double2 ys = ybytes == 0 ? __ldg(p.ybuf[ycur] + gd) : preD(0)[e];
         const double2 k0 = to_d2(preX(1)[nd * ES + w]), k2 = to_d2(preX(2)[nd * ES + w]);
         const double2 k3 = to_d2(preX(3)[nd * ES + w]), k4 = to_d2(preX(4)[nd * ES + w]);
         double2 y4 = cfma(ys, k0, cf[15]);
@@ -659,34 +549,210 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
         }
       }
     }
-    if (MIXED && s == 5) emax = sqrt(emax);
-    if (s == 5) {
-      unsigned long long bits = (unsigned long long)__double_as_longlong(emax);
-      for (int off = 16; off > 0; off >>= 1) {
-        const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
-        bits = o > bits ? o : bits;
-      }
-      // One atomic per CTA: a single error word takes every CTA's maximum,
-      // so per-warp atomics would serialise tens of thousands of updates.
-      if ((tid & 31) == 0) wmax[tid >> 5] = bits;
-      __syncthreads();
-      if (tid == 0) {
-        unsigned long long m = wmax[0];
+  }
+}
+
+// The RKF45 stage-5 error of a CTA: the maximum over its threads' emax, one
+// atomicMax on the bit pattern of the control block's error word.
+template <bool MIXED, int BT>
+__device__ __forceinline__ void tile_error_max(const TileParams &p, double emax, unsigned long long *wmax) {
+  const int tid = threadIdx.x;
+  if (MIXED) emax = sqrt(emax);
+    unsigned long long bits = (unsigned long long)__double_as_longlong(emax);
+    for (int off = 16; off > 0; off >>= 1) {
+      const unsigned long long o = __shfl_xor_sync(0xffffffffu, bits, off);
+      bits = o > bits ? o : bits;
+    }
+    // One atomic per CTA: a single error word takes every CTA's maximum,
+    // so per-warp atomics would serialise tens of thousands of updates.
+    if ((tid & 31) == 0) wmax[tid >> 5] = bits;
+    __syncthreads();
+    if (tid == 0) {
+      unsigned long long m = wmax[0];
 #pragma unroll
-        for (int w = 1; w < (BT / 32); ++w) m = wmax[w] > m ? wmax[w] : m;
-        if (m) atomicMax(&p.ctl->err_bits, m);
-      }
+      for (int w = 1; w < (BT / 32); ++w) m = wmax[w] > m ? wmax[w] : m;
+      if (m) atomicMax(&p.ctl->err_bits, m);
+    }
+}
+
+// New filter flags of a tile's nodes after the stage that writes the new
+// state (RK4 stage 3, RKF45 stage 5).
+template <int N, int KT, bool MIXED, int BT>
+__device__ __forceinline__ void tile_flags(const TileParams &p, const typename TileArith<MIXED>::TX *Us, long long n0,
+                                           int nt_here, int ycur) {
+  using S = TileShape<N, MIXED, KT, BT>;
+  using TX = typename TileArith<MIXED>::TX;
+  const HeomConsts &c = p.c;
+  if (!(c.filtered && ((p.mode == kModeRk4 && p.stage == 3) || (p.mode == kModeRkf45 && p.stage == 5)))) return;
+  // Below the tolerance -> inactive, above -> active, equal -> unchanged
+  // (hierarchy_integrator.cc:2827-2850, :2359-2384).
+  __syncthreads();
+  const int ap = p.mode == kModeRkf45 ? ycur : p.act_par;
+  tile_filter_flags(reinterpret_cast<const unsigned char *>(Us), (int)sizeof(TX), N, S::NP, nt_here,
+                    p.act[ap] + n0, p.act[ap ^ 1] + n0, c.filter_tol, BT / 32);
+}
+
+
+// KT = terms per site (K + 1) under PHI's identity site map.
+// One tile (NT consecutive nodes of one hierarchy) of one stage.  The caller
+// has initialised the two mbarriers at the start of shared memory and passes
+// the phase parity each is at.  Returns 1 when the tile was skipped before
+// any copy was issued (RKF45 run finished), 0 when both barriers completed a
+// phase (barrier 1 with 0 bytes when p.npre == 0), -1 after a bounded wait gave up
+// (err_flag set; the caller must stop).
+template <int N, int KT, bool MIXED, int BT = kTileThreads>
+__device__ __forceinline__ int tile_body(const TileParams &p, long long tile, unsigned char *smem_raw,
+                                         uint32_t par0, uint32_t par1) {
+  using S = TileShape<N, MIXED, KT, BT>;
+  using Lay = TileLayout<N, MIXED, KT, BT>;
+  using TX = typename std::conditional<MIXED, float2, double2>::type;
+  using R = typename std::conditional<MIXED, float, double>::type;
+  constexpr int E = S::E, P = S::P, NT = S::NT, ES = Lay::ES;
+  const HeomConsts &c = p.c;
+  constexpr int T = N * KT;  // PHI's identity site map: K+1 terms per site
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + Lay::kBars);
+  TX *Xs = reinterpret_cast<TX *>(smem_raw + Lay::kX);   // NT*ES
+  TX *Us = reinterpret_cast<TX *>(smem_raw + Lay::kU);   // NT*EU (column stride NP)
+  unsigned char *PreBase = smem_raw + Lay::kPre;
+  // Byte offsets of the prefetched epilogue operands.  Every loop over them
+  // is unrolled so the offsets stay in registers.
+  uint32_t pre_off[kMaxPre];
+  size_t tail = Lay::kPre;
+  {
+    uint32_t acc_off = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      pre_off[b] = acc_off;
+      if (b < p.npre) acc_off += ((uint32_t)NT * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b] + 127) / 128 * 128;
+    }
+    tail += acc_off;
+  }
+  TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
+  double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
+  double *coef = deph + NT;                                         // 24
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
+  R *cn = reinterpret_cast<R *>(wmax + (BT / 32));                          // NT*T |next prefactor|
+  R *cp = cn + NT * T;                                              // NT*T prev scale
+  R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
+  R *mats = ccr + 2 * T;                                            // E    Matsubara factor per element
+  int *ids = reinterpret_cast<int *>(mats + E);                     // NT*2T element offsets
+  int *nts = ids + NT * 2 * T;                                      // NT*T
+  unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
+  unsigned char *pj = pi + P;
+
+  const int tid = threadIdx.x;
+  int ycur = 0;
+  if (p.mode == kModeRkf45) {
+    if (*(volatile int *)&p.ctl->done) return 1;  // uniform across the grid
+    ycur = p.ctl->ycur;
+    if (tid < 24) coef[tid] = p.ctl->coef[tid];
+  }
+  const long long n0 = tile * NT;
+  if (n0 >= c.M) return 1;
+  // Filtering: the flags of the current state are p.act[ap], ap = ycur
+  // (RKF45) or p.act_par; the launch that writes the new state (RK4 stage 3,
+  // RKF45 stage 5 -- the candidate, kept on accept) writes its flags to
+  // p.act[ap ^ 1].  Both are recomputed from the parameters where used, so
+  // nothing of it stays live across the tile.
+  auto act_idx = [&]() { return p.mode == kModeRkf45 ? ycur : p.act_par; };
+  const int nt_here = (int)((c.M - n0) < NT ? (c.M - n0) : NT);
+  const TX *xin;
+  if (p.mode == kModeRkf45 && p.stage == 0)
+    xin = MIXED ? static_cast<const TX *>(p.y32buf[ycur]) : reinterpret_cast<const TX *>(p.ybuf[ycur]);
+  else
+    xin = static_cast<const TX *>(p.x);
+
+  // ---- t = 0: bulk prefetch of the tile's contiguous ranges ----
+  if (tid == 0) {
+    const uint32_t xbytes = (uint32_t)(nt_here * ES * Lay::XB);
+    mbar_expect_tx(&bars[0], xbytes);
+    bulk_g2s(Xs, xin + n0 * ES, xbytes, &bars[0]);
+    uint32_t pbytes = 0;
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b)
+      if (b < p.npre) pbytes += (uint32_t)(nt_here * (p.pre_bytes[b] == 16 ? E : ES) * p.pre_bytes[b]);
+    // Arrives on barrier 1 in every tile (with 0 bytes when nothing is
+    // prefetched), so its phase advances once per tile like barrier 0's.
+    mbar_expect_tx(&bars[1], pbytes);
+#pragma unroll
+    for (int b = 0; b < kMaxPre; ++b) {
+      if (b >= p.npre) break;
+      if (p.pre_bytes[b] == 0) continue;  // read from global in the epilogue
+      const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
+      if (b == 0 && p.mode == kModeRkf45)
+        src = static_cast<const unsigned char *>(p.pre_bytes[0] == 8 ? p.y32buf[ycur] : (const void *)p.ybuf[ycur]);
+      const int stride = p.pre_bytes[b] == 16 ? E : ES;
+      const uint32_t bytes = (uint32_t)(nt_here * stride * p.pre_bytes[b]);
+      bulk_g2s(PreBase + pre_off[b], src + (size_t)n0 * stride * p.pre_bytes[b], bytes, &bars[1]);
     }
   }
-  if (flag_stage()) {
-    // New flags of the state just written (hierarchy_integrator.cc:2827-2850,
-    // :2359-2384): below the tolerance -> inactive, above -> active, equal ->
-    // unchanged.
-    __syncthreads();
-    const int ap = act_idx();
-    tile_filter_flags(reinterpret_cast<const unsigned char *>(Us), (int)sizeof(TX), N, NP, nt_here,
-                      p.act[ap] + n0, p.act[ap ^ 1] + n0, c.filter_tol, BT / 32);
+  // A real Hamiltonian (every in-scope workload) is kept as E reals in the
+  // same buffer, halving the products of A = H X.
+  const bool hreal = c.h_real;
+  R *Hr = reinterpret_cast<R *>(Hs);
+  if (hreal) {
+    for (int i = tid; i < E; i += BT) Hr[i] = (R)__ldg(c.H + i).x;
+  } else {
+    for (int i = tid; i < E; i += BT) Hs[i] = from_d2<TX>(__ldg(c.H + i));
   }
+  for (int i = tid; i < E; i += BT) mats[i] = (R)__ldg(c.mats_elem + i);
+  for (int i = tid; i < P; i += BT) {
+    pi[i] = __ldg(c.pair_i + i);
+    pj[i] = __ldg(c.pair_j + i);
+  }
+  const int W = c.L + 2;
+  const int tile_terms = nt_here * T;
+  // Per (node, term): neighbour ids scaled to element offsets of the stage
+  // input (-1 when absent), occupation, and the prefactor magnitudes for that
+  // occupation, so the pair loop reads shared memory only.
+  const uint8_t *act_in = c.filtered ? p.act[act_idx()] : nullptr;
+  for (int q = tid; q < tile_terms; q += BT) {
+    const int nd = q / T, t = q - nd * T;
+    const int nx = __ldg(c.next + n0 * T + q), pv = __ldg(c.prev + n0 * T + q);
+    const int nt = __ldg(c.mi + n0 * T + q);
+    // An inactive neighbour contributes nothing (the DoNext / DoPrevious
+    // overrides of IndependentBathAdaptiveTruncation, hierarchy_updater.cc:256-303).
+    const bool nx_on = nx >= 0 && (!act_in || __ldg(act_in + nx));
+    const bool pv_on = pv >= 0 && (!act_in || __ldg(act_in + pv));
+    ids[nd * 2 * T + t] = nx_on ? nx * ES : -1;
+    ids[nd * 2 * T + T + t] = pv_on ? pv * ES : -1;
+    nts[q] = nt;
+    cn[q] = (R)__ldg(c.sq_next + t * W + nt);
+    cp[q] = (R)__ldg(c.sq_prev + t * W + nt);
+  }
+  for (int t = tid; t < T; t += BT) {
+    const double2 ct = __ldg(c.corr + t);
+    ccr[2 * t] = (R)ct.x;
+    ccr[2 * t + 1] = (R)ct.y;
+  }
+  __syncthreads();  // barrier init and metadata visible
+  if (tid < nt_here) {
+    double d = 0.0;
+    for (int t = 0; t < T; ++t) d += nts[tid * T + t] * __ldg(c.nu + t);
+    deph[tid] = d;
+  }
+  const long long polls0 = c.first_wait_polls == 0 ? kMaxPolls : (c.first_wait_polls < 0 ? 0 : c.first_wait_polls);
+  bool ok = mbar_wait_bounded(&bars[0], par0, polls0);
+  __syncthreads();  // deph visible
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) atomicOr(c.err_flag, 1);
+    // Drain this tile's own copies with the built-in limit, so no copy is
+    // still writing into shared memory when the CTA stops.
+    mbar_wait_bounded(&bars[0], par0);
+    if (p.npre > 0) mbar_wait_bounded(&bars[1], par1);
+    return -1;
+  }
+
+  tile_pairs<N, KT, MIXED, BT>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
+  ok = p.npre == 0 || mbar_wait_bounded(&bars[1], par1);
+  if (!__syncthreads_and(ok)) {
+    if (tid == 0) atomicOr(c.err_flag, 1);
+    return -1;
+  }
+  double emax = 0.0;
+  tile_epilogue<N, KT, MIXED, BT>(p, Xs, Us, PreBase, pre_off, coef, wmax, tile, n0, nt_here, ycur, emax);
+  if (p.mode == kModeRkf45 && p.stage == 5) tile_error_max<MIXED, BT>(p, emax, wmax);
+  tile_flags<N, KT, MIXED, BT>(p, Us, n0, nt_here, ycur);
   return 0;
 }
 
