@@ -60,6 +60,7 @@ struct HeomConsts {
   const double2 *H;      // N*N Hamiltonian
   const double2 *corr;   // T   c_t
   const double *nu;      // T   dephasing rate of term t
+  const double *deph_node;  // M (+2 slack): sum_t n_t nu_t of every node
   const double *sq_next; // T*(L+2): |next prefactor| for n_t = 0..L+1
   const double *sq_prev; // T*(L+2): prev scale for n_t = 0..L+1
   const int32_t *term_site;  // T: independent -> site, diagonal/full -> bath

@@ -1,10 +1,10 @@
 // heom_tile.cu -- tiled Liouvillian-apply / RK-stage kernel for one
-// IndependentBath hierarchy: one launch per stage over the hierarchy's tiles;
-// the tile itself is tile_body in heom_tile_body.cuh.
+// IndependentBath hierarchy: one persistent launch per stage whose CTAs walk
+// the hierarchy's tiles; the pair loop and the epilogue of a tile are
+// tile_pairs / tile_epilogue of heom_tile_body.cuh.
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <cstdlib>
 #include <cstring>
 
 #include "heom_tile_body.cuh"
@@ -24,25 +24,6 @@ template <int N, bool MIXED>
 struct TileBlock {
   static constexpr int threads = (MIXED && N == 24) ? 320 : kTileThreads;
 };
-
-// Experiment switch during development: PHI_TILE_PIPELINE=0 selects the
-// one-tile-per-CTA kernel.
-bool tile_pipeline_enabled() {
-  static const bool on = [] {
-    const char *v = std::getenv("PHI_TILE_PIPELINE");
-    return !(v && v[0] == '0');
-  }();
-  return on;
-}
-
-template <int N, int KT, bool MIXED>
-__global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
-                                  TileMinBlocks<KT, MIXED, TileBlock<N, MIXED>::threads>::value)
-    heom_tile_kernel(TileParams p) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  tile_init_barriers(smem_raw);
-  tile_body<N, KT, MIXED, TileBlock<N, MIXED>::threads>(p, blockIdx.x, smem_raw, 0u, 0u);
-}
 
 // ---- persistent pipelined kernel ----
 //
@@ -64,13 +45,15 @@ struct PipeLayout {
   static constexpr int RB = MIXED ? 4 : 8;  // bytes of the arithmetic type
   static constexpr size_t r16(size_t b) { return (b + 15) / 16 * 16; }
   static constexpr size_t r128(size_t b) { return (b + 127) / 128 * 128; }
-  // One slot: the tile's X, then its next ids, prev ids (int32) and
-  // occupations (uint8), each copied from the 16-byte aligned window around
-  // the tile's records (up to 3 ids / 15 bytes of slack on either side).
+  // One slot: the tile's X, then its next ids, prev ids (int32),
+  // occupations (uint8) and dephasing rates (double), each copied from the
+  // 16-byte aligned window around the tile's records (up to 3 ids, 15
+  // bytes or 1 rate of slack on either side).
   static constexpr size_t kSlotX = r128((size_t)S::NT * ES * XB);
   static constexpr size_t kSlotIds = r16(((size_t)S::NT * T + 8) * 4);
   static constexpr size_t kSlotMi = r16((size_t)S::NT * T + 32);
-  static constexpr size_t kSlot = r128(kSlotX + 2 * kSlotIds + kSlotMi);
+  static constexpr size_t kSlotDeph = r16(((size_t)S::NT + 2) * 8);  // per-node dephasing rates
+  static constexpr size_t kSlot = r128(kSlotX + 2 * kSlotIds + kSlotMi + kSlotDeph);
   static constexpr size_t kSlots = 128;                       // after the 3 mbarriers
   static constexpr size_t kUs = kSlots + 2 * kSlot;           // derivative tile
   static constexpr size_t kPre = kUs + r128((size_t)S::NT * S::EU * XB);
@@ -85,7 +68,7 @@ size_t pipe_smem(int T, int L, int npre, const int *pre_bytes) {
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   const int W = L + 2;
   b += (size_t)S::E * Lay::XB;                                        // H
-  b += (size_t)(S::NT + 24 + BT / 32 + T) * sizeof(double);           // deph, coef, warp maxima, rates
+  b += (size_t)(36 + BT / 32) * sizeof(double);                       // coef (FP64, FP32), warp maxima
   b += (size_t)(2 * S::NT * T + 2 * T + S::E + 2 * T * W) * Lay::RB;  // cn, cp, c_t, mats, prefactor tables
   b += (size_t)(S::NT * 3 * T) * sizeof(int);                         // ids, occupations
   b += 2 * S::P + 16;
@@ -123,11 +106,9 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
   }
   const int W = c.L + 2;
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                           // E
-  double *deph = reinterpret_cast<double *>(Hs + E);                          // NT
-  double *coef = deph + NT;                                                   // 24
-  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // BT / 32
-  double *rate = reinterpret_cast<double *>(wmax + BT / 32);                  // T
-  R *cn = reinterpret_cast<R *>(rate + T);                                    // NT*T
+  double *coef = reinterpret_cast<double *>(Hs + E);                          // 24, then 24 floats
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 36);  // BT / 32
+  R *cn = reinterpret_cast<R *>(wmax + BT / 32);                              // NT*T
   R *cp = cn + NT * T;                                                        // NT*T
   R *ccr = cp + NT * T;                                                       // 2T
   R *mats = ccr + 2 * T;                                                      // E
@@ -147,7 +128,11 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
   int ycur = 0;
   if (p.mode == kModeRkf45) {
     ycur = p.ctl->ycur;
-    if (tid < 24) coef[tid] = p.ctl->coef[tid];
+    if (tid < 24) {
+      const double v = p.ctl->coef[tid];
+      coef[tid] = v;
+      reinterpret_cast<float *>(coef + 24)[tid] = (float)v;
+    }
   }
   const bool hreal = c.h_real;
   R *Hr = reinterpret_cast<R *>(Hs);
@@ -165,7 +150,6 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
     const double2 ct = __ldg(c.corr + t);
     ccr[2 * t] = (R)ct.x;
     ccr[2 * t + 1] = (R)ct.y;
-    rate[t] = __ldg(c.nu + t);
   }
   for (int q = tid; q < T * W; q += BT) {
     sqn[q] = (R)__ldg(c.sq_next + q);
@@ -192,13 +176,15 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
     unsigned char *b = smem_raw + Lay::kSlots + (size_t)s * Lay::kSlot;
     const long long q0 = n0 * T, q1 = q0 + (long long)nt * T;
     const long long a4 = q0 & ~3ll, e4 = (q1 + 3) & ~3ll, a16 = q0 & ~15ll, e16 = (q1 + 15) & ~15ll;
+    const long long a2 = n0 & ~1ll, e2 = (n0 + nt + 1) & ~1ll;
     const uint32_t xbytes = (uint32_t)(nt * ES * Lay::XB), idbytes = (uint32_t)((e4 - a4) * 4),
-                   mibytes = (uint32_t)(e16 - a16);
-    mbar_expect_tx(&bars[s], xbytes + 2 * idbytes + mibytes);
+                   mibytes = (uint32_t)(e16 - a16), dbytes = (uint32_t)((e2 - a2) * 8);
+    mbar_expect_tx(&bars[s], xbytes + 2 * idbytes + mibytes + dbytes);
     bulk_g2s(b, xin + n0 * ES, xbytes, &bars[s]);
     bulk_g2s(b + Lay::kSlotX, c.next + a4, idbytes, &bars[s]);
     bulk_g2s(b + Lay::kSlotX + Lay::kSlotIds, c.prev + a4, idbytes, &bars[s]);
     bulk_g2s(b + Lay::kSlotX + 2 * Lay::kSlotIds, c.mi + a16, mibytes, &bars[s]);
+    bulk_g2s(b + Lay::kSlotX + 2 * Lay::kSlotIds + Lay::kSlotMi, c.deph_node + a2, dbytes, &bars[s]);
   };
   // Thread 0: the epilogue operands of `tile`.
   auto issue_pre = [&](long long tile) {
@@ -241,14 +227,15 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
       break;
     }
     // Per (node, term): neighbour element offsets (-1 when absent or
-    // inactive), occupation and the prefactor magnitudes for it; per node:
-    // the dephasing rate.
+    // inactive), occupation and the prefactor magnitudes for it.
     const unsigned char *sb = smem_raw + Lay::kSlots + (size_t)s * Lay::kSlot;
     const TX *Xs = reinterpret_cast<const TX *>(sb);
     const int q0 = (int)((n0 * T) & 15);
     const int *nx_s = reinterpret_cast<const int *>(sb + Lay::kSlotX) + (q0 & 3);
     const int *pv_s = reinterpret_cast<const int *>(sb + Lay::kSlotX + Lay::kSlotIds) + (q0 & 3);
     const uint8_t *mi_s = sb + Lay::kSlotX + 2 * Lay::kSlotIds + q0;
+    const double *deph =
+        reinterpret_cast<const double *>(sb + Lay::kSlotX + 2 * Lay::kSlotIds + Lay::kSlotMi) + (n0 & 1);
     for (int q = tid; q < nt_here * T; q += BT) {
       const int nd = q / T, t = q - nd * T;
       const int nx = nx_s[q], pv = pv_s[q], nt = mi_s[q];
@@ -259,11 +246,6 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
       nts[q] = nt;
       cn[q] = sqn[t * W + nt];
       cp[q] = sqp[t * W + nt];
-    }
-    if (tid < nt_here) {
-      double d = 0.0;
-      for (int t = 0; t < T; ++t) d += mi_s[tid * T + t] * rate[t];
-      deph[tid] = d;
     }
     __syncthreads();
     tile_pairs<N, KT, MIXED, BT>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
@@ -318,25 +300,16 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
   using S = TileShape<N, MIXED, KT, BT>;
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
-  if (tile_pipeline_enabled()) {
-    const size_t smem_max = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, kMaxPre, max_bytes);
-    auto kern = heom_tile_pipe_kernel<N, KT, MIXED>;
-    static thread_local int configured[kSmemLimitDevices] = {};
-    cudaError_t e = raise_smem_limit(kern, smem_max, configured);
-    if (e != cudaSuccess) return e;
-    const size_t smem = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, p.npre, p.pre_bytes);
-    const int cap = persistent_grid((const void *)kern, BT, smem);
-    if (cap <= 0) return cudaErrorInvalidConfiguration;
-    const long long grid = tiles < cap ? tiles : cap;
-    kern<<<(unsigned)grid, BT, smem, stream>>>(p);
-    return cudaGetLastError();
-  }
-  const size_t smem_max = tile_smem<N, KT, MIXED, BT>(p.c.T, kMaxPre, max_bytes);
-  auto kern = heom_tile_kernel<N, KT, MIXED>;
+  const size_t smem_max = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, kMaxPre, max_bytes);
+  auto kern = heom_tile_pipe_kernel<N, KT, MIXED>;
   static thread_local int configured[kSmemLimitDevices] = {};
   cudaError_t e = raise_smem_limit(kern, smem_max, configured);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)tiles, BT, tile_smem<N, KT, MIXED, BT>(p.c.T, p.npre, p.pre_bytes), stream>>>(p);
+  const size_t smem = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, p.npre, p.pre_bytes);
+  const int cap = persistent_grid((const void *)kern, BT, smem);
+  if (cap <= 0) return cudaErrorInvalidConfiguration;
+  const long long grid = tiles < cap ? tiles : cap;
+  kern<<<(unsigned)grid, BT, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -425,7 +398,9 @@ TileParams tile_params_for(const StageLaunch &L) {
       p.pre[0] = L.y;
       p.npre = 1;
     } else if (L.stage == 1 || L.stage == 2) {
-      p.pre[0] = L.y;
+      // mixed: the complex64 copy y32 feeds the complex64 stage input
+      p.pre[0] = mixed ? (const void *)L.y32 : (const void *)L.y;
+      p.pre_bytes[0] = mixed ? 8 : 16;
       p.pre[1] = L.acc;
       p.npre = 2;
     } else if (L.stage == 3) {

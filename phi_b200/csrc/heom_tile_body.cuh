@@ -394,6 +394,8 @@ __device__ __forceinline__ void tile_pairs(const HeomConsts &c, const typename T
 // stage combine) from the derivative tile Us and the prefetched operands at
 // PreBase + pre_off[b]; the RKF45 stage-5 error of this thread's elements is
 // folded into emax (max of |y4 - y5|, or of its square in mixed precision).
+// coef holds the 24 RKF45 coefficients in FP64 followed by the same 24 in
+// FP32.
 template <int N, int KT, bool MIXED, int BT>
 __device__ __forceinline__ void tile_epilogue(const TileParams &p, const typename TileArith<MIXED>::TX *Xs,
                                               typename TileArith<MIXED>::TX *Us, const unsigned char *PreBase,
@@ -477,8 +479,17 @@ __device__ __forceinline__ void tile_epilogue(const TileParams &p, const typenam
       const int nd = e / E, w = e - nd * E;
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const double2 kv = to_d2(Us[uix(e)]);
-      if (s == 0) {  // FP64: pre = {} (y is the input); MIXED: pre = {y}
-        const double2 ys = MIXED ? preD(0)[e] : to_d2(Xs[nd * ES + w]);
+      if (MIXED && s < 3) {
+        // Mixed: the complex64 stage input y32 + a k in FP32 (stage 0: y32
+        // is the input; stages 1-2: pre = {y32, acc}); the accumulator in
+        // FP64 (stage 0: pre = {y}).
+        const float af = (float)p.a_next;
+        const TX kx = Us[uix(e)];
+        const TX ys = s == 0 ? Xs[nd * ES + w] : preX(0)[nd * ES + w];
+        out[gx] = mk<TX>(fmaf((float)kx.x, af, (float)ys.x), fmaf((float)kx.y, af, (float)ys.y));
+        st_stream(p.acc + gd, cfma((s == 0 ? preD(0) : preD(1))[e], kv, p.w_acc));
+      } else if (s == 0) {  // FP64: pre = {} (y is the input)
+        const double2 ys = to_d2(Xs[nd * ES + w]);
         out[gx] = from_d2<TX>(cfma(ys, kv, p.a_next));
         st_stream(p.acc + gd, cfma(ys, kv, p.w_acc));
       } else if (s < 3) {  // pre = {y, acc}
@@ -509,7 +520,27 @@ __device__ __forceinline__ void tile_epilogue(const TileParams &p, const typenam
       const long long gd = (n0 + nd) * E + w, gx = (n0 + nd) * ES + w;
       const TX kx = Us[uix(e)];
       const double2 kv = to_d2(kx);
-      if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; stage 0: y is the input
+      if (MIXED && s < 5) {
+        // Mixed stages 0-4: the complex64 stage input X_{s+1} = y32 + sum b k
+        // in FP32 throughout (it is stored in complex64; an FP64 combine
+        // rounded to it differs by an ulp of complex64).  pre = {y32, k_0 ..
+        // k_{s-1}}; stage 0: y32 is the input.
+        const float *cff = reinterpret_cast<const float *>(coef + 24);
+        const TX ys = s == 0 ? Xs[nd * ES + w] : preX(0)[nd * ES + w];
+        st_stream(static_cast<TX *>(p.k[s]) + gx, kx);
+        const int row = s * (s + 1) / 2;
+        float xr = ys.x, xi = ys.y;
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+          if (r < s) {
+            const TX kr = preX(1 + r)[nd * ES + w];
+            xr = fmaf((float)kr.x, cff[row + r], xr);
+            xi = fmaf((float)kr.y, cff[row + r], xi);
+          }
+        xr = fmaf((float)kx.x, cff[row + s], xr);
+        xi = fmaf((float)kx.y, cff[row + s], xi);
+        out[gx] = mk<TX>(xr, xi);
+      } else if (s < 5) {  // pre = {y, k_0 .. k_{s-1}}; stage 0: y is the input
         const double2 ys = s == 0 ? to_d2(Xs[nd * ES + w])
                            : (ybytes == 0 ? __ldg(p.ybuf[ycur] + gd)
                                           : (ybytes == 8 ? to_d2(preX(0)[nd * ES + w]) : preD(0)[e]));
@@ -629,8 +660,8 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   }
   TX *Hs = reinterpret_cast<TX *>(smem_raw + tail);                 // E
   double *deph = reinterpret_cast<double *>(Hs + E);                // NT (8-aligned: E*8 or E*16)
-  double *coef = deph + NT;                                         // 24
-  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 24);  // per-warp maxima
+  double *coef = deph + NT;                                         // 24, then 24 floats
+  unsigned long long *wmax = reinterpret_cast<unsigned long long *>(coef + 36);  // per-warp maxima
   R *cn = reinterpret_cast<R *>(wmax + (BT / 32));                          // NT*T |next prefactor|
   R *cp = cn + NT * T;                                              // NT*T prev scale
   R *ccr = cp + NT * T;                                             // 2T   c_t (re, im)
@@ -645,7 +676,11 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   if (p.mode == kModeRkf45) {
     if (*(volatile int *)&p.ctl->done) return 1;  // uniform across the grid
     ycur = p.ctl->ycur;
-    if (tid < 24) coef[tid] = p.ctl->coef[tid];
+    if (tid < 24) {
+      const double v = p.ctl->coef[tid];
+      coef[tid] = v;
+      reinterpret_cast<float *>(coef + 24)[tid] = (float)v;
+    }
   }
   const long long n0 = tile * NT;
   if (n0 >= c.M) return 1;
@@ -728,7 +763,7 @@ __device__ __forceinline__ int tile_body(const TileParams &p, long long tile, un
   __syncthreads();  // barrier init and metadata visible
   if (tid < nt_here) {
     double d = 0.0;
-    for (int t = 0; t < T; ++t) d += nts[tid * T + t] * __ldg(c.nu + t);
+    for (int t = 0; t < T; ++t) d = fma((double)nts[tid * T + t], __ldg(c.nu + t), d);
     deph[tid] = d;
   }
   const long long polls0 = c.first_wait_polls == 0 ? kMaxPolls : (c.first_wait_polls < 0 ? 0 : c.first_wait_polls);
@@ -764,7 +799,7 @@ inline size_t tile_smem(int T, int npre, const int *pre_bytes) {
   for (int i = 0; i < npre; ++i)
     b += ((size_t)S::NT * (pre_bytes[i] == 16 ? S::E : Lay::ES) * pre_bytes[i] + 127) / 128 * 128;
   b += (size_t)S::E * Lay::XB;
-  b += (size_t)(S::NT + 24 + BT / 32) * sizeof(double);  // deph, coef, warp maxima
+  b += (size_t)(S::NT + 36 + BT / 32) * sizeof(double);  // deph, coef (FP64 and FP32), warp maxima
   b += (size_t)(2 * S::NT * T + 2 * T + S::E) * Lay::XB / 2;  // cn, cp, ccr, mats in the arithmetic type
   b += (size_t)(S::NT * 3 * T) * sizeof(int);
   b += 2 * S::P + 16;

@@ -354,6 +354,7 @@ extern "C" int phi_gpu_batch_rk4(phi_batch *batch, double dt, int64_t steps, phi
     }
     e = cudaGraphInstantiate(&batch->graph, g, 0);
     cudaGraphDestroy(g);
+    if (e == cudaSuccess) e = cudaGraphUpload(batch->graph, s);  // not on the first launch
     if (e != cudaSuccess) return batch->cuda_fail(e, "batch graph instantiate");
     batch->graph_grid = grid;
   }

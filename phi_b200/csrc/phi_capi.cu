@@ -76,6 +76,19 @@ namespace phi {
 
 // Builds the per-term / per-element constant tables and the device copy of
 // the problem (see HeomConsts).
+namespace {
+// Dephasing rate of every node, sum_t n_t nu_t in term order (the tile
+// kernels' per-node dephasing, DoDephasing, hierarchy_updater.h:71-75).
+__global__ void node_dephasing_kernel(const uint8_t *__restrict__ mi, const double *__restrict__ nu, long long M,
+                                      int T, double *__restrict__ out) {
+  for (long long n = blockIdx.x * (long long)blockDim.x + threadIdx.x; n < M; n += (long long)gridDim.x * blockDim.x) {
+    double d = 0.0;
+    for (int t = 0; t < T; ++t) d = fma((double)mi[n * T + t], nu[t], d);
+    out[n] = d;
+  }
+}
+}  // namespace
+
 int setup_constants(phi_ctx *ctx) {
   const phi_problem_desc &d = ctx->desc;
   const int N = d.num_states, nb = d.num_baths, K1 = d.num_matsubara_terms;
@@ -195,6 +208,16 @@ int setup_constants(phi_ctx *ctx) {
   chk(upload(cb.pair_j, pj, s));
   chk(cb.err_flag.alloc(sizeof(int)));
   chk(cudaMemsetAsync(cb.err_flag.ptr, 0, sizeof(int), s));
+  // Per-node dephasing rates, 2 doubles of slack: the tile kernels copy a
+  // tile's rates as a 16-byte aligned window.
+  const long long Mn = ctx->hier.M;
+  chk(cb.deph_node.alloc((size_t)(Mn + 2) * sizeof(double)));
+  chk(cudaMemsetAsync(cb.deph_node.ptr, 0, (size_t)(Mn + 2) * sizeof(double), s));
+  if (e == cudaSuccess && T > 0 && Mn > 0) {
+    node_dephasing_kernel<<<(unsigned)std::min<long long>((Mn + 255) / 256, 4096), 256, 0, s>>>(
+        ctx->hier.mi.as<uint8_t>(), cb.nu.as<double>(), Mn, T, cb.deph_node.as<double>());
+    chk(cudaGetLastError());
+  }
   chk(cudaStreamSynchronize(s));
   if (e != cudaSuccess) return cuda_fail(ctx, e, "constant upload");
 
@@ -223,6 +246,7 @@ int setup_constants(phi_ctx *ctx) {
   c.H = cb.H.as<double2>();
   c.corr = cb.corr.as<double2>();
   c.nu = cb.nu.as<double>();
+  c.deph_node = cb.deph_node.as<double>();
   c.sq_next = cb.sq_next.as<double>();
   c.sq_prev = cb.sq_prev.as<double>();
   c.term_site = cb.term_site.as<int32_t>();

@@ -15,7 +15,7 @@
 // Device copies of the per-term / per-element constants (HeomConsts points here).
 struct PhiConstBuffers {
   phi::DeviceBuffer H, corr, nu, sq_next, sq_prev, term_site, site_ptr, site_terms,
-      mats_elem, bath_V, mats_bath, pair_i, pair_j, err_flag;
+      mats_elem, bath_V, mats_bath, pair_i, pair_j, err_flag, deph_node;
 };
 
 struct phi_ctx {

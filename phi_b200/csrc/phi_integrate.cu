@@ -191,6 +191,8 @@ cudaError_t capture(cudaStream_t s, F &&body, cudaGraphExec_t *exec) {
   if (e != cudaSuccess) return e;
   e = cudaGraphInstantiate(exec, graph, 0);
   cudaGraphDestroy(graph);
+  // Upload now, on the capturing stream, so the first launch does not pay it.
+  if (e == cudaSuccess) e = cudaGraphUpload(*exec, s);
   return e;
 }
 

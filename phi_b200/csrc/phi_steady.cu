@@ -206,6 +206,7 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     }
     cudaError_t ei = cudaGraphInstantiate(&ctx->bicg_graph, graph, 0);
     cudaGraphDestroy(graph);
+    if (ei == cudaSuccess) ei = cudaGraphUpload(ctx->bicg_graph, s);  // not on the first launch
     if (ei != cudaSuccess) return steady_err(ctx, ei, "instantiate");
     ctx->bicg_ell = ell;
   }
