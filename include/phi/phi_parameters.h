@@ -16,9 +16,7 @@
 #include <string>
 
 #include "../phi_b200.h"
-
-typedef double Float;
-typedef std::complex<double> Complex;
+#include "numeric_types.h"
 
 // Reduced Planck constant in [cm-1*ps] and Boltzmann constant in [cm-1/K]
 // (phi_parameters.h:13-16).
@@ -67,12 +65,14 @@ struct PHI_API PhiParameters {
 
   Float temperature;
 
+  Float *kappa;  // accepted for compatibility (PHI declares it; no path reads it)
   Float *gamma;
   Float *lambda;
   Float *bath_coupling_op;
   int *multiple_independent_bath_indices;
 
   Complex *initial_density_matrix;
+  Complex *spectrum_initial_density_matrix;  // spectra are out of scope; freed like PHI's
 
   Float integration_time;
   Float timestep;
@@ -87,6 +87,7 @@ struct PHI_API PhiParameters {
   std::string output_filename;
   std::string restart_input_filename;
   std::string restart_output_filename;
+  std::string restart_backup_filename;  // accepted for compatibility
 
   bool is_truncated_system;
   bool use_time_local_truncation;
@@ -98,8 +99,19 @@ struct PHI_API PhiParameters {
   bool is_restarted;
   bool has_kappa;
 
+  // Eigen data of the Hamiltonian (PHI's steady-state initial guess reads
+  // them when present; accepted for compatibility, not owned).
+  Complex *hamiltonian_eigenvectors, *hamiltonian_eigenvalues;
+  bool are_e_vecs_present;
+  bool are_e_vals_present;
+
   int bicgstab_ell;
-  int num_threads;  // accepted for compatibility; the GPU path ignores it
+  // CPU thread controls of PHI's pthread runtime: accepted for
+  // compatibility, the GPU path ignores them.
+  int num_threads;
+  int num_cores;
+  int *cpuaffinity;
+  bool stupid_hierarchy_partition;
   bool are_parameters_valid;
   RunMethod run_method;
 
@@ -116,6 +128,9 @@ struct PHI_API PhiParameters {
   void SetDefaults();
   bool FileExists(const char *filename);
   void FixIncompatibleCombinations();
+  // Presence and range checks of phi_parameters.cc:890-932 (PHI itself never
+  // calls it); clears are_parameters_valid with PHI's messages on stderr.
+  void CheckParameters();
   void ReadCommandLine(int num_args, char *argv[]);
   void ReadInputFile(std::string parameter_file);
   void Write(std::ofstream *out, long long num_matrices);

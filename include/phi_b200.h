@@ -162,6 +162,9 @@ PHI_API int phi_gpu_destroy(phi_ctx *ctx);
 /* Hierarchy size: M nodes, T = num_baths * (K+1) terms, N states. */
 PHI_API int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num_terms,
                  int32_t *num_states);
+/* Number of bath coupling terms (PHI's num_bath_couplings); T / num_baths
+ * is K+1. */
+PHI_API int phi_gpu_num_baths(const phi_ctx *ctx, int32_t *num_baths);
 
 /* Node table built on the device, copied to host buffers of M*T int32 each
  * (any may be NULL): multi_index[i*T + t] = n_t of node i; next[i*T + t] =
@@ -181,9 +184,10 @@ PHI_API int phi_gpu_get_state(const phi_ctx *ctx, double *state);
 PHI_API int phi_gpu_get_active(const phi_ctx *ctx, uint8_t *flags);
 
 /* Time-local truncation sums Q_m of the current state, host buffer of
- * 2*N*N*N doubles: one complex column-major N x N matrix per bath (time-local
- * truncation runs on PHI's identity site map, so num_baths = N); all zero
- * when it is off.  Zero after create, set_state and reset. */
+ * 2*num_baths*N*N doubles: one complex column-major N x N matrix per bath
+ * (num_baths = N for independent baths, which time-local truncation needs on
+ * PHI's identity site map); all zero when it is off.  Zero after create,
+ * set_state and reset. */
 PHI_API int phi_gpu_get_time_local(const phi_ctx *ctx, double *q);
 
 /* The Hamiltonian the next stage starts from, host buffer of 2*N*N doubles

@@ -279,7 +279,7 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
   const int T = c->T;
   c->M = oracle_node_count(T, c->trunc);
   c->filter_tol = p->filter_tolerance;
-  c->tl = p->time_local && p->bath_kind == ORACLE_BATH_INDEPENDENT;
+  c->tl = p->time_local;
   c->active = (unsigned char *)malloc((size_t)(c->M > 0 ? c->M : 1));
   if (c->active) memset(c->active, 1, (size_t)(c->M > 0 ? c->M : 1));
   if (c->M <= 0) { free(c); return NULL; }
@@ -631,6 +631,15 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
      * uses the bare (unnormalised) operators whatever is_rho_normalized says. */
     for (int m = 0; m < c->nb; ++m)
       for (int n = 0; n < E; ++n) d[n] -= c->same[m * E + n] * r[n];
+    /* DiagonalBath::DoTimelocal (:93-104) on the deepest tier, whose next
+     * list is empty: temp = -i (Q_m rho - rho Q_m^+), d += (-i)(V_j - V_i) temp. */
+    if (c->tl && c->tier[i] == c->trunc - 1) {
+      for (int m = 0; m < c->nb; ++m) {
+        hemm_right(N, cx(0, -1), r, c->tlq + (size_t)m * E, 0, temp);
+        hemm_left(N, cx(0, 1), r, c->tlqa + (size_t)m * E, 1, temp);
+        for (int n = 0; n < E; ++n) d[n] += c->nextop[m * E + n] * temp[n];
+      }
+    }
     for (int j = 0; j < np.num_next; ++j) {
       const cplx *op = c->nextop + term_bath(c, np.next_term[j]) * E;
       const cplx *rn = rho + (int64_t)np.next_id[j] * E;
@@ -652,6 +661,17 @@ static void apply_node(const oracle_ctx *c, int64_t i, const cplx *rho, cplx *ou
       hemm_left(N, -1, r, S, 1, temp);
       hemm_left(N, -1, S, temp, 1, d);
       hemm_right(N, 1, S, temp, 1, d);
+    }
+    /* FullBath::DoTimelocal (:28-44) on the deepest tier:
+     * temp = -i (Q_m rho - rho Q_m^+), d += (-i V_m) temp - temp (-i V_m). */
+    if (c->tl && c->tier[i] == c->trunc - 1) {
+      for (int m = 0; m < c->nb; ++m) {
+        const cplx *B = c->nextop + m * E;
+        hemm_right(N, cx(0, -1), r, c->tlq + (size_t)m * E, 0, temp);
+        hemm_left(N, cx(0, 1), r, c->tlqa + (size_t)m * E, 1, temp);
+        hemm_right(N, 1, temp, B, 1, d);
+        hemm_left(N, -1, temp, B, 1, d);
+      }
     }
     for (int j = 0; j < np.num_next; ++j) {
       const cplx *B = c->nextop + term_bath(c, np.next_term[j]) * E;
@@ -762,7 +782,16 @@ static void tl_update(const oracle_ctx *c, double h) {
       cplx *Q = c->tlqk + ((size_t)m * K1 + k) * E;
       const cplx cf = h * c->corr[m * K1 + k];
       const cplx damp = k == 0 ? cx(exp(-c->gamma[m] * h), 0) : cx(exp(-nu * k * h), 0);
-      Q[m * N + m] += cf;  /* AddIndependentBathOperator at (m, m) */
+      /* AddIndependentBathOperator at (m, m); AddDiagonalBathOperator on the
+       * diagonal; AddFullBathOperator (Axpy) on every element
+       * (hierarchy.cc:218-233, :289-300). */
+      if (c->kind == ORACLE_BATH_DIAGONAL) {
+        for (int d = 0; d < N; ++d) Q[d * N + d] += cf * c->bath[(size_t)m * N + d];
+      } else if (c->kind == ORACLE_BATH_FULL) {
+        for (int e = 0; e < E; ++e) Q[e] = cf * c->bath[(size_t)m * E + e] + Q[e];
+      } else {
+        Q[m * N + m] += cf;
+      }
       gemm(N, damp, Ua, Q, 0, tmp);
       gemm(N, 1, tmp, U, 0, Q);
     }

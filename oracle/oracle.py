@@ -160,7 +160,7 @@ class Oracle:
         ft = float(getattr(p, "filter_tolerance", 0.0) or 0.0)
         pr.filter_tolerance = ft if pr.bath_kind == 0 else 0.0
         # Time-local truncation, restated for independent baths.
-        pr.time_local = 1 if (getattr(p, "use_time_local_truncation", False) and pr.bath_kind == 0) else 0
+        pr.time_local = 1 if getattr(p, "use_time_local_truncation", False) else 0
         # Annealing Hamiltonian H(t) = f_x(t/T) H_X + f_z(t/T) H_Z.
         if getattr(p, "transverse_hamiltonian", None) is not None:
             pr.h_x = arr(_colmajor(np.asarray(p.transverse_hamiltonian, np.complex128)))

@@ -284,6 +284,43 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
             group_sync<GROUP>(g);
           }
         }
+        if (tlf_s[0]) {
+          // Time-local truncation on the deepest tier, DiagonalBath /
+          // FullBath::DoTimelocal (hierarchy_updater.cc:28-44, :93-104):
+          // W = Q_b X - X Q_b^+, then -[V_b, W] for every bath b.
+          for (int b = 0; b < c.nb; ++b) {
+            const double2 *Q = c.tl_q + (size_t)b * E;
+            group_sync<GROUP>(g);  // W is reused
+            for (int e = lane; e < E; e += GROUP) {
+              const int i = e % N, j = e / N;
+              double2 w = make_double2(0.0, 0.0);
+              for (int k = 0; k < N; ++k) {
+                w = c_add(w, c_mul(__ldg(Q + i + k * N), Xs[k + j * N]));
+                w = c_sub(w, c_mul(Xs[i + k * N], c_conj(__ldg(Q + j + k * N))));
+              }
+              W[e] = w;
+            }
+            group_sync<GROUP>(g);
+            if (KIND == kDiagonal) {
+              const double *V = c.bath_V + (size_t)b * N;
+              for (int e = lane; e < E; e += GROUP) {
+                const int i = e % N, j = e / N;
+                NB[e] = c_axpy(NB[e], W[e], -(__ldg(V + i) - __ldg(V + j)));
+              }
+            } else {
+              const double *V = c.bath_V + (size_t)b * E;
+              for (int e = lane; e < E; e += GROUP) {
+                const int i = e % N, j = e / N;
+                double2 vw = make_double2(0.0, 0.0);
+                for (int k = 0; k < N; ++k) {
+                  vw = c_axpy(vw, W[k + j * N], __ldg(V + i + k * N));
+                  vw = c_axpy(vw, W[i + k * N], -__ldg(V + k + j * N));
+                }
+                NB[e] = c_sub(NB[e], vw);
+              }
+            }
+          }
+        }
       }
     }
     group_sync<GROUP>(g);

@@ -78,8 +78,23 @@ __global__ void __launch_bounds__(kTlThreads) tl_kernel(TlLaunch p) {
       const int t = m * K1 + k;
       for (int e = tid; e < E; e += kTlThreads) Qs[e] = qk[(size_t)k * E + e];
       __syncthreads();
-      if (tid == 0) {  // + h c_{m,k} |m><m|
-        const double2 ct = c.corr[t];
+      // + h c_{m,k} times the bath operator: |m><m| for independent baths,
+      // diag(V_m) for diagonal ones, V_m for full ones (AddIndependent /
+      // AddDiagonal / AddFullBathOperator, hierarchy.cc:218-233, :289-300).
+      const double2 ct = c.corr[t];
+      if (c.kind == kDiagonal) {
+        for (int d = tid; d < N; d += kTlThreads) {
+          const double v = c.bath_V[(size_t)m * N + d];
+          Qs[d + d * N].x += h * ct.x * v;
+          Qs[d + d * N].y += h * ct.y * v;
+        }
+      } else if (c.kind == kFull) {
+        for (int e = tid; e < E; e += kTlThreads) {
+          const double v = c.bath_V[(size_t)m * E + e];
+          Qs[e].x = fma(h * ct.x, v, Qs[e].x);
+          Qs[e].y = fma(h * ct.y, v, Qs[e].y);
+        }
+      } else if (tid == 0) {
         Qs[m + m * N].x += h * ct.x;
         Qs[m + m * N].y += h * ct.y;
       }

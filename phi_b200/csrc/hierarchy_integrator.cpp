@@ -29,9 +29,9 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
                   "field arrays (2 samples or more)");
   if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
     return reject("Hilbert-space truncation is outside this library's scope");
-  if (p.use_time_local_truncation &&
-      (p.is_diagonal_bath_coupling || p.is_full_bath_coupling || p.is_multiple_independent_baths))
-    return reject("time-local truncation is built for independent baths on PHI's identity site map");
+  if (p.use_time_local_truncation && p.is_multiple_independent_baths && !p.is_diagonal_bath_coupling &&
+      !p.is_full_bath_coupling)
+    return reject("time-local truncation with independent baths needs PHI's identity site map");
   if (p.is_spectrum_calculation) return reject("spectrum calculations are outside this library's scope");
   const bool steady = p.run_method == BICGSTAB || p.run_method == BICGSTABL || p.run_method == BICGSTABU;
   if (p.initial_density_matrix == nullptr && !steady && !p.is_restarted)
@@ -368,10 +368,18 @@ void HierarchyIntegrator::WriteRestartIfAsked(double timestep) {
 }
 
 Complex *HierarchyIntegrator::density_matrix() {
+  // hilbert_space_size x hilbert_space_size, like PHI's (its truncated
+  // systems return rho in the full space, hierarchy_integrator.cc:177-191).
   const int N = parameters_->num_states;
-  Complex *rho = new Complex[(size_t)N * N];
-  const Complex *src = has_result_ ? result_ : parameters_->initial_density_matrix;
-  for (int i = 0; i < N * N; ++i) rho[i] = src ? src[i] : Complex(0, 0);
+  const int H = std::max(N, parameters_->hilbert_space_size);
+  Complex *rho = new Complex[(size_t)H * H];
+  for (int i = 0; i < H * H; ++i) rho[i] = Complex(0, 0);
+  if (has_result_) {
+    for (int j = 0; j < N; ++j)
+      for (int i = 0; i < N; ++i) rho[i + (size_t)j * H] = result_[i + (size_t)j * N];
+  } else if (parameters_->initial_density_matrix) {
+    for (int i = 0; i < H * H; ++i) rho[i] = parameters_->initial_density_matrix[i];
+  }
   return rho;
 }
 

@@ -334,18 +334,16 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
     return fail(nullptr, PHI_E_INVALID, "filter_tolerance must be finite and >= 0");
   if (d.time_local != 0 && d.time_local != 1)
     return fail(nullptr, PHI_E_INVALID, "time_local must be 0 or 1");
-  if (d.time_local) {
-    // PHI's diagonal-bath time-local term reads its operator table with the
-    // full-matrix stride (hierarchy_updater.cc:92-104 against the per-state
-    // layout of hierarchy.cc:185-197), and its independent-bath matrices put
-    // c at (b, b) whatever site bath b couples to (hierarchy.cc:298-300);
-    // only the independent identity map has a defined result.
-    bool identity = d.bath_kind == PHI_BATH_INDEPENDENT && d.num_baths == N;
+  if (d.time_local && d.bath_kind == PHI_BATH_INDEPENDENT) {
+    // PHI's independent-bath matrices put c at (b, b) whatever site bath b
+    // couples to (hierarchy.cc:298-300), while its DoTimelocal works on site
+    // b's row and column: only the identity site map is consistent.
+    bool identity = d.num_baths == N;
     if (identity && d.bath_sites)
       for (int b = 0; b < d.num_baths; ++b) identity = identity && d.bath_sites[b] == b;
     if (!identity)
       return fail(nullptr, PHI_E_INVALID,
-                  "time-local truncation is built for independent baths on PHI's identity site map "
+                  "time-local truncation with independent baths needs PHI's identity site map "
                   "(bath j on |j><j|)");
   }
 
@@ -488,6 +486,12 @@ extern "C" int phi_gpu_dims(const phi_ctx *ctx, int64_t *num_nodes, int32_t *num
   return PHI_OK;
 }
 
+extern "C" int phi_gpu_num_baths(const phi_ctx *ctx, int32_t *num_baths) {
+  if (!ctx || !num_baths) return PHI_E_INVALID;
+  *num_baths = ctx->desc.num_baths;
+  return PHI_OK;
+}
+
 extern "C" int phi_gpu_get_node_table(const phi_ctx *cctx, int32_t *multi_index, int32_t *next,
                                       int32_t *prev) {
   phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
@@ -578,7 +582,7 @@ extern "C" int phi_gpu_get_hamiltonian(const phi_ctx *cctx, double *h) {
 extern "C" int phi_gpu_get_time_local(const phi_ctx *cctx, double *q) {
   phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
   if (!ctx || !q) return PHI_E_INVALID;
-  const size_t n = (size_t)ctx->desc.num_states * ctx->desc.num_states * ctx->desc.num_states;
+  const size_t n = (size_t)ctx->desc.num_baths * ctx->desc.num_states * ctx->desc.num_states;
   if (!ctx->c.time_local) {
     std::memset(q, 0, n * sizeof(double2));
     return PHI_OK;

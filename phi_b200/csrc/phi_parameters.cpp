@@ -168,9 +168,12 @@ PhiParameters::PhiParameters() {
   final_hamiltonian_field = nullptr;
   final_hamiltonian_field_size = 0;
   minimum_field_change = 0.01;
-  gamma = lambda = bath_coupling_op = nullptr;
+  kappa = gamma = lambda = bath_coupling_op = nullptr;
   multiple_independent_bath_indices = nullptr;
   initial_density_matrix = nullptr;
+  spectrum_initial_density_matrix = nullptr;
+  hamiltonian_eigenvectors = hamiltonian_eigenvalues = nullptr;
+  cpuaffinity = nullptr;
   SetDefaults();
 }
 
@@ -180,11 +183,13 @@ PhiParameters::~PhiParameters() {
   delete[] initial_annealing_hamiltonian;
   delete[] initial_hamiltonian_field;
   delete[] final_hamiltonian_field;
+  delete[] kappa;
   delete[] gamma;
   delete[] lambda;
   delete[] bath_coupling_op;
   delete[] multiple_independent_bath_indices;
   delete[] initial_density_matrix;
+  delete[] spectrum_initial_density_matrix;
 }
 
 // Defaults of PhiParameters::SetDefaults (phi_parameters.cc:9-88).
@@ -218,8 +223,15 @@ void PhiParameters::SetDefaults() {
   is_restarted = false;
   restart_output_time = 0;
   has_kappa = false;
+  are_e_vecs_present = false;
+  are_e_vals_present = false;
   bicgstab_ell = 2;
   num_threads = 1;
+  num_cores = 1;
+  stupid_hierarchy_partition = false;
+  restart_input_filename.clear();
+  restart_output_filename.clear();
+  restart_backup_filename.clear();
   are_parameters_valid = true;
   run_method = NONE;
   precision = 0;
@@ -451,6 +463,29 @@ void PhiParameters::ReadInputFile(std::string parameter_file) {
 }
 
 // PhiParameters::FixIncompatibleCombinations (phi_parameters.cc:786-888).
+void PhiParameters::CheckParameters() {
+  const std::string e = "INPUT ERROR ";
+  auto bad = [&](const char *msg) {
+    std::cerr << e << msg << "\n";
+    are_parameters_valid = false;
+  };
+  if (num_states <= 0) bad("NumStates must be > 0");
+  if (hierarchy_truncation_level < 1) bad("HierarchyTruncation must be > 0");
+  if (num_bath_couplings <= 0) bad("NumCouplingTerms must be > 0");
+  if (num_matsubara_terms < 0) bad("NumMatsubaraTerms must be >= 0");
+  // A static Hamiltonian, or both annealing Hamiltonians.  (PHI's test asks
+  // for both kinds at once, which no valid input has.)
+  if (time_indepenent_hamiltonian == nullptr &&
+      (initial_annealing_hamiltonian == nullptr || final_annealing_hamiltonian == nullptr))
+    bad("Hamiltonian must be specified");
+  if (gamma == nullptr) bad("Gamma values must be specified");
+  if (lambda == nullptr) bad("Lambda values must be specified");
+  if (initial_density_matrix == nullptr && spectrum_initial_density_matrix == nullptr && is_spectrum_calculation)
+    bad("Initial state must be specified");
+  if (use_time_local_truncation && is_restarted)
+    bad("Restarting time-local calculations truncation not implemented.");
+}
+
 void PhiParameters::FixIncompatibleCombinations() {
   are_parameters_valid = !(time_indepenent_hamiltonian == nullptr &&
                            (initial_annealing_hamiltonian == nullptr ||
@@ -459,6 +494,16 @@ void PhiParameters::FixIncompatibleCombinations() {
     std::cout << "Invalid parameters, no Hamiltonian?.\n";
     run_method = BROKENINPUT;
     return;
+  }
+  // Annealing without field samples: the transverse field ramps 1 -> 0 and
+  // the longitudinal one 0 -> 1 over the run (phi_parameters.cc:801-815).
+  if (initial_annealing_hamiltonian != nullptr && initial_hamiltonian_field == nullptr) {
+    initial_hamiltonian_field_size = 2;
+    initial_hamiltonian_field = new Float[2]{1.0, 0.0};
+  }
+  if (initial_annealing_hamiltonian != nullptr && final_hamiltonian_field == nullptr) {
+    final_hamiltonian_field_size = 2;
+    final_hamiltonian_field = new Float[2]{0.0, 1.0};
   }
   if ((run_method == RKF45 || run_method == RKF45SPECTRUM || run_method == BICGSTAB ||
        run_method == BICGSTABL || run_method == BICGSTABU) &&

@@ -206,6 +206,9 @@ class Hierarchy:
         self.num_nodes = M.value
         self.num_terms = T.value
         self.n = N.value
+        nb = ctypes.c_int32()
+        self._check(self.lib.phi_gpu_num_baths(self.ctx, ctypes.byref(nb)))
+        self.num_baths = nb.value
 
     def _check(self, code):
         capi.check(code, self.ctx)
@@ -259,10 +262,10 @@ class Hierarchy:
         return out.astype(bool)
 
     def time_local(self) -> np.ndarray:
-        """Time-local truncation sums Q_m, (N, N, N) complex in PHI's
-        column-major storage (element [m, j, i] = Q_m[i, j]; one matrix per
-        bath, num_baths = N on the identity site map); zeros when off."""
-        nb = self.n
+        """Time-local truncation sums Q_m, (num_baths, N, N) complex in PHI's
+        column-major storage (element [m, j, i] = Q_m[i, j]); zeros when
+        off."""
+        nb = self.num_baths
         out = np.zeros(2 * nb * self.n * self.n, np.float64)
         self._check(self.lib.phi_gpu_get_time_local(self.ctx, out.ctypes.data))
         return out.view(np.complex128).reshape(nb, self.n, self.n)

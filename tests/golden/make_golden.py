@@ -256,6 +256,20 @@ TIMELOCAL_CASES = [
     ("rand_n3_k2_t4/rkf45/filter1e-3", "random_problem",
      dict(kind="independent", n=3, matsubara=2, truncation=4, seed=2), "rkf45", 0.001, 0.05, 1e-3),
     ("frenkel7_L2/rkf45", "config:frenkel7", dict(depth=2), "rkf45", 0.001, 0.05, 0.0),
+    # correlated (diagonal) and full bath couplings: DiagonalBath / FullBath
+    # DoTimelocal and the NoHierarchy updaters of a single tier
+    ("diag_n3_b2_k2_t3/rk4", "random_problem", dict(kind="diagonal", n=3, matsubara=2, truncation=3, baths=2,
+                                                     seed=4), "rk4", 0.001, 0.05, 0.0),
+    ("diag_n3_b2_k2_t3/rkf45", "random_problem", dict(kind="diagonal", n=3, matsubara=2, truncation=3, baths=2,
+                                                       seed=4), "rkf45", 0.001, 0.05, 0.0),
+    ("full_n3_b2_k2_t3/rk4", "random_problem", dict(kind="full", n=3, matsubara=2, truncation=3, baths=2,
+                                                     seed=5), "rk4", 0.001, 0.05, 0.0),
+    ("full_n3_b2_k2_t3/rkf45", "random_problem", dict(kind="full", n=3, matsubara=2, truncation=3, baths=2,
+                                                       seed=5), "rkf45", 0.001, 0.05, 0.0),
+    ("diag_n2_b2_k2_t1/rk4", "random_problem", dict(kind="diagonal", n=2, matsubara=2, truncation=1, baths=2,
+                                                     seed=6), "rk4", 0.001, 0.05, 0.0),
+    ("full_n3_b2_k1_t1/rkf45", "random_problem", dict(kind="full", n=3, matsubara=1, truncation=1, baths=2,
+                                                       seed=7), "rkf45", 0.001, 0.05, 0.0),
 ]
 
 

@@ -26,11 +26,11 @@ def test_unknown_method_is_rejected(tmp_path):
 
 
 def test_time_local_outside_identity_map_is_rejected(tmp_path):
-    """TimeLocal with correlated (diagonal) bath couplings: PHI's term for
-    them reads its operator table with the wrong stride, so the library
-    refuses the input instead of guessing."""
+    """TimeLocal with independent baths on another site map
+    (DiagonalCouplingIndices): PHI adds c at (b, b) whatever site bath b
+    couples to, so the library refuses the input instead of guessing."""
     import cases
-    p = cases.random_problem("diagonal", n=3, matsubara=2, truncation=3, seed=1)
-    text = O.param_file_text(p) + "TimeLocal=1\n"
+    p = cases.random_problem("independent", n=3, matsubara=2, truncation=3, seed=1)
+    text = O.param_file_text(p) + "TimeLocal=1\nDiagonalCouplingIndices:\n0,2,1\n"
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
         Hierarchy.from_file(_write(tmp_path, text), "rkf45")

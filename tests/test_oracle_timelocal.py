@@ -6,9 +6,10 @@ the reference build, the whole final state from the restart file the same
 run wrote (6 significant digits, small hierarchies) and, for RKF45, the sums
 over k of the stored Q_{m,k} that file ends with.  PHI advances
 Q_{m,k} <- d_k U^+ (Q_{m,k} + h c_{m,k} |m><m|) U with U = I - i H h
-(hierarchy.cc:229-341) along the stage times, and the deepest tier adds
+(hierarchy.cc:229-341) along the stage times (with diag(V_m) or V_m in place
+of |m><m| for diagonal and full couplings), and the deepest tier adds
 -sum_m [V_m, Q_m rho - rho Q_m^+] in place of its next terms
-(hierarchy_updater.cc:171-190).
+(hierarchy_updater.cc:28-44, :93-104, :171-190).
 """
 import json
 import os
@@ -112,11 +113,12 @@ def test_chunked_rk4_keeps_time_local_state():
     assert np.abs(b - one).max() <= 1e-14 * np.abs(one).max()
 
 
-@pytest.mark.parametrize("kind", ["diagonal", "full"])
-def test_time_local_outside_identity_map_is_rejected(kind):
-    """PHI's diagonal-bath term reads its operator table with the wrong
-    stride; only the independent identity map has a defined result."""
-    p = cases.random_problem(kind, n=3, matsubara=2, truncation=3, seed=1)
+def test_time_local_outside_identity_map_is_rejected():
+    """Independent baths on another site map: PHI adds c at (b, b) whatever
+    site bath b couples to (hierarchy.cc:298-300), so the library refuses the
+    input instead of guessing.  (Diagonal and full couplings are built.)"""
+    p = cases.random_problem("independent", n=3, matsubara=2, truncation=3, seed=1)
+    p.bath_sites = np.array([0, 2, 1], np.int32)
     p.use_time_local_truncation = True
     with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
         Hierarchy(p)
