@@ -55,7 +55,8 @@ class PHI_API HierarchyIntegrator {
   long long accepted_ = 0;
   double residual_ = 0;
   bool has_result_ = false;
-  Complex *result_ = nullptr;
+  Complex *result_ = nullptr;  // result_size_ x result_size_ (the full Hilbert space)
+  int result_size_ = 0;
 
   bool Prepare();
   void RunRk4(std::ofstream &out);

@@ -120,6 +120,15 @@ typedef struct {
   int32_t longitudinal_field_size;   /* >= 2 */
   double integration_time;           /* T (Time); > 0 */
   double minimum_field_change;       /* MinimumFieldChange (PHI's default 0.01) */
+  /* Hilbert-space truncation (hilbert_space_size, is_truncated_system;
+   * HilbertSpaceTruncator, hilbert_space_truncator.cc:34-134): when
+   * hilbert_space_size F > num_states k, hamiltonian, initial_density_matrix
+   * and the full bath operators in coupling are given in the F-dimensional
+   * space and the hierarchy runs in the basis of the lowest k eigenvectors of
+   * the Hamiltonian (V^+ A V); phi_gpu_get_rho0_full returns V rho_0 V^+.
+   * Static, real symmetric Hamiltonians; full bath couplings (or a single
+   * tier without time-local truncation).  0 = no truncation. */
+  int32_t hilbert_space_size;
 } phi_problem_desc;
 
 typedef struct phi_ctx phi_ctx;
@@ -265,6 +274,14 @@ enum {
  * (PHI_E_NO_CONVERGENCE).  FP64 in every precision. */
 PHI_API int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
                                  const double *guess, phi_solve_stats *stats);
+
+/* rho_0 in the full Hilbert space, V rho_0 V^+ (UnTruncate,
+ * hilbert_space_truncator.cc:82-95; hierarchy_integrator.cc:177-191): host
+ * buffer of 2*F*F doubles, F = hilbert_space_size (the same as
+ * phi_gpu_get_rho0 without truncation). */
+PHI_API int phi_gpu_get_rho0_full(const phi_ctx *ctx, double *rho0);
+/* F, the Hilbert-space size of the problem (num_states without truncation). */
+PHI_API int phi_gpu_hilbert_space_size(const phi_ctx *ctx, int32_t *size);
 
 /* Time carried by the context (advanced by the integrators). */
 PHI_API int phi_gpu_get_time(const phi_ctx *ctx, double *time);

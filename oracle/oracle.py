@@ -23,6 +23,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libheom_oracle.so")
 REF_DRIVER = os.path.join(HERE, "_ref", "ref_driver")
+# The reference built in BLAS mode (oracle/refbuild/Makefile `blas`): the
+# configuration its Hilbert-space truncation is correct in.
+REF_DRIVER_BLAS = os.path.join(HERE, "_ref_blas", "ref_driver")
 
 
 class _Problem(ctypes.Structure):
@@ -365,6 +368,11 @@ def param_file_text(p, timestep=None, t_end=None, output_min_step=None, rkf45_to
     lines = [f"OutputFile={output_file}", "verbose=-2",
              f"hbar={_fmt(p.hbar)}", f"kB={_fmt(p.boltzmann_constant)}",
              f"NumStates={n}"]
+    hs = int(getattr(p, "hilbert_space_size", 0) or 0)
+    if hs > n:
+        # Hilbert-space truncation: matrices in the full space (phi_parameters.cc:219-238)
+        lines.append(f"HilbertSpaceSize={hs}")
+        n = hs
     if getattr(p, "transverse_hamiltonian", None) is not None:
         # Annealing Hamiltonian (phi_parameters.cc:363-441).
         for key, M, fkey, f in (("TransverseHamiltonian", p.transverse_hamiltonian, "TransverseField",
@@ -423,15 +431,16 @@ def ref_available() -> bool:
     return os.path.exists(REF_DRIVER)
 
 
-def run_reference(p, method: str, threads: int = 1, timeout: float = 600.0, **kw):
-    """Runs the reference integrator; returns (rho_0 as N x N complex, seconds)."""
-    n = int(p.num_states)
+def run_reference(p, method: str, threads: int = 1, timeout: float = 600.0, driver: str = None, **kw):
+    """Runs the reference integrator; returns (rho_0 as N x N complex, seconds)
+    (F x F, F = hilbert_space_size, under Hilbert-space truncation)."""
+    n = max(int(p.num_states), int(getattr(p, "hilbert_space_size", 0) or 0))
     with tempfile.TemporaryDirectory() as d:
         prm = os.path.join(d, "in.prm")
         out = os.path.join(d, "rho.txt")
         with open(prm, "w") as f:
             f.write(param_file_text(p, **kw))
-        subprocess.run([REF_DRIVER, "run", prm, method, str(threads), out], check=True,
+        subprocess.run([driver or REF_DRIVER, "run", prm, method, str(threads), out], check=True,
                        timeout=timeout, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE)
         secs = float(open(out).read().split("\n")[0].split()[1])
         return parse_rho_file(out, n), secs

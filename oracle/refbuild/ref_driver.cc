@@ -53,7 +53,10 @@ int RunIntegration(int argc, char** argv) {
     std::fprintf(stderr, "ref_driver: invalid parameters\n");
     return 2;
   }
-  const int n = parameters.num_states;
+  // density_matrix() is hilbert_space_size^2 (UnTruncate under Hilbert-space
+  // truncation; num_states^2 otherwise).
+  const int n = parameters.hilbert_space_size > parameters.num_states ? parameters.hilbert_space_size
+                                                                        : parameters.num_states;
   double t0 = WallSeconds();
   HierarchyIntegrator integrator(&parameters);
   integrator.Launch();

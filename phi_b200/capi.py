@@ -72,6 +72,7 @@ class PhiProblemDesc(ctypes.Structure):
         ("longitudinal_field_size", c_int32),
         ("integration_time", c_double),
         ("minimum_field_change", c_double),
+        ("hilbert_space_size", c_int32),
     ]
 
 
@@ -117,6 +118,8 @@ SIGNATURES = [
     ("phi_gpu_create_from_file", c_int, [c_char_p, c_char_p, c_int32, c_int32, POINTER(c_void_p)]),
     ("phi_gpu_destroy", c_int, [c_void_p]),
     ("phi_gpu_dims", c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32), POINTER(c_int32)]),
+    ("phi_gpu_get_rho0_full", c_int, [c_void_p, c_void_p]),
+    ("phi_gpu_hilbert_space_size", c_int, [c_void_p, POINTER(c_int32)]),
     ("phi_gpu_num_baths", c_int, [c_void_p, POINTER(c_int32)]),
     ("phi_gpu_get_node_table", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_set_state", c_int, [c_void_p, c_void_p]),

@@ -27,8 +27,7 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
                     p.initial_hamiltonian_field_size < 2 || p.final_hamiltonian_field_size < 2))
     return reject("an annealing Hamiltonian needs TransverseHamiltonian, LongitudinalHamiltonian and both "
                   "field arrays (2 samples or more)");
-  if (p.is_truncated_system || p.hilbert_space_size > p.num_states)
-    return reject("Hilbert-space truncation is outside this library's scope");
+
   if (p.use_time_local_truncation && p.is_multiple_independent_baths && !p.is_diagonal_bath_coupling &&
       !p.is_full_bath_coupling)
     return reject("time-local truncation with independent baths needs PHI's identity site map");
@@ -68,6 +67,8 @@ int descriptor_from_parameters(const PhiParameters &p, phi_problem_desc *d, std:
   d->max_nodes = 0;
   d->filter_tolerance = p.filter_tolerance;  // already 0 for diagonal / full baths
   d->time_local = p.use_time_local_truncation ? 1 : 0;  // already 0 for the steady-state methods
+  // Hilbert-space truncation: the matrices above are given in the full space.
+  d->hilbert_space_size = p.hilbert_space_size > p.num_states ? p.hilbert_space_size : 0;
   if (annealing) {
     d->hamiltonian = nullptr;
     d->annealing_h_x = reinterpret_cast<const double *>(p.initial_annealing_hamiltonian);
@@ -185,9 +186,13 @@ void HierarchyIntegrator::Run(int, int, RunMethod method) {
   else if (method == RKF45) RunRkf45(out);
   else RunSteadyState(out);
   if (status_ == PHI_OK || (steady && status_ == PHI_E_NO_CONVERGENCE)) {
+    // rho_0 in the full Hilbert space (UnTruncate under truncation).
+    int32_t F = N;
+    phi_gpu_hilbert_space_size(ctx_, &F);
     delete[] result_;
-    result_ = new Complex[(size_t)N * N];
-    phi_gpu_get_rho0(ctx_, reinterpret_cast<double *>(result_));
+    result_ = new Complex[(size_t)F * F];
+    result_size_ = F;
+    phi_gpu_get_rho0_full(ctx_, reinterpret_cast<double *>(result_));
     has_result_ = true;
   }
 }
@@ -375,8 +380,9 @@ Complex *HierarchyIntegrator::density_matrix() {
   Complex *rho = new Complex[(size_t)H * H];
   for (int i = 0; i < H * H; ++i) rho[i] = Complex(0, 0);
   if (has_result_) {
-    for (int j = 0; j < N; ++j)
-      for (int i = 0; i < N; ++i) rho[i + (size_t)j * H] = result_[i + (size_t)j * N];
+    const int R = std::min(result_size_, H);
+    for (int j = 0; j < R; ++j)
+      for (int i = 0; i < R; ++i) rho[i + (size_t)j * H] = result_[i + (size_t)j * result_size_];
   } else if (parameters_->initial_density_matrix) {
     for (int i = 0; i < H * H; ++i) rho[i] = parameters_->initial_density_matrix[i];
   }

@@ -23,6 +23,7 @@
 #include "heom_anneal.h"
 #include <cfloat>
 #include "phi_context.h"
+#include "phi_truncation.h"
 
 using phi::DeviceBuffer;
 
@@ -290,6 +291,27 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
     return fail(nullptr, PHI_E_INVALID, "unknown bath_kind");
   if (d.precision != PHI_PREC_FP64 && d.precision != PHI_PREC_MIXED)
     return fail(nullptr, PHI_E_INVALID, "unknown precision");
+  if (d.hilbert_space_size != 0 && d.hilbert_space_size < N)
+    return fail(nullptr, PHI_E_INVALID, "hilbert_space_size cannot be less than num_states");
+  if (d.hilbert_space_size > N) {
+    // Hilbert-space truncation: restate the problem in the lowest num_states
+    // eigenvectors of the Hamiltonian, then build an ordinary context.
+    if (d.hilbert_space_size > 1024) return fail(nullptr, PHI_E_INVALID, "hilbert_space_size must be <= 1024");
+    if (!d.hamiltonian || !d.initial_density_matrix)
+      return fail(nullptr, PHI_E_INVALID, "hamiltonian and initial_density_matrix are required");
+    const int F = d.hilbert_space_size;
+    for (int k = 0; k < 2 * F * F; ++k)
+      if (!std::isfinite(d.hamiltonian[k]) || !std::isfinite(d.initial_density_matrix[k]))
+        return fail(nullptr, PHI_E_INVALID, "non-finite value in the Hamiltonian or the initial density matrix");
+    phi::TruncatedProblem t;
+    std::string err;
+    if (phi::truncate_problem(d, &t, &err) != 0) return fail(nullptr, PHI_E_INVALID, err);
+    const int rc = phi_gpu_create(&t.desc, out);
+    if (rc != PHI_OK) return rc;
+    (*out)->hilbert_full = F;
+    (*out)->trunc_basis = std::move(t.basis);
+    return PHI_OK;
+  }
   const bool annealing = d.annealing_h_x != nullptr;
   if ((!d.hamiltonian && !annealing) || !d.initial_density_matrix || !d.gamma || !d.lambda)
     return fail(nullptr, PHI_E_INVALID, "hamiltonian, initial_density_matrix, gamma and lambda are required");
@@ -626,6 +648,24 @@ extern "C" int phi_gpu_get_state(const phi_ctx *cctx, double *state) {
   if (!ctx || !state) return PHI_E_INVALID;
   PHI_CUDA(ctx, cudaMemcpyAsync(state, ctx->y.ptr, ctx->state_bytes(), cudaMemcpyDeviceToHost, ctx->stream));
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_hilbert_space_size(const phi_ctx *ctx, int32_t *size) {
+  if (!ctx || !size) return PHI_E_INVALID;
+  *size = ctx->hilbert_full > 0 ? ctx->hilbert_full : ctx->desc.num_states;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_rho0_full(const phi_ctx *cctx, double *rho0) {
+  phi_ctx *ctx = const_cast<phi_ctx *>(cctx);
+  if (!ctx || !rho0) return PHI_E_INVALID;
+  const int k = ctx->desc.num_states;
+  if (ctx->hilbert_full <= k) return phi_gpu_get_rho0(ctx, rho0);
+  std::vector<double> rk(2 * (size_t)k * k);
+  const int rc = phi_gpu_get_rho0(ctx, rk.data());
+  if (rc != PHI_OK) return rc;
+  phi::untruncate(ctx->hilbert_full, k, ctx->trunc_basis.data(), rk.data(), rho0);
   return PHI_OK;
 }
 

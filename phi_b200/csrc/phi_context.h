@@ -92,6 +92,11 @@ struct phi_ctx {
   void *host_ctl = nullptr;        // pinned copy of the control block
   long long graph_launches = 0;    // step graphs launched so far
 
+  // Hilbert-space truncation: the full size F and the kept eigenvectors V
+  // (F x num_states, real); hilbert_full == num_states without truncation.
+  int hilbert_full = 0;
+  std::vector<double> trunc_basis;
+
   double time = 0.0;
   std::string error;
   ~phi_ctx() {

@@ -60,6 +60,11 @@ class PhiParameters:
     transverse_field: Optional[np.ndarray] = None
     longitudinal_field: Optional[np.ndarray] = None
     minimum_field_change: float = 0.01
+    # Hilbert-space truncation: > num_states gives the Hamiltonian, the
+    # initial density matrix and the full bath operators in this larger space
+    # (PHI's HilbertSpaceSize); the hierarchy keeps the lowest num_states
+    # eigenvectors of the Hamiltonian.  0 = no truncation.
+    hilbert_space_size: int = 0
 
     @property
     def bath_kind(self) -> int:
@@ -110,8 +115,12 @@ def problem_desc(p: PhiParameters, precision: int, device: int, max_nodes: int, 
     """phi_problem_desc of a PhiParameters; the arrays it points to are
     appended to keep_list (the caller keeps them alive)."""
     n = int(p.num_states)
+    hs = int(p.hilbert_space_size or 0)
+    if hs > n:
+        n = hs  # matrices are given in the full space
     d = capi.PhiProblemDesc()
-    d.num_states = n
+    d.hilbert_space_size = hs
+    d.num_states = int(p.num_states)
     d.num_baths = int(p.num_bath_couplings)
     d.num_matsubara_terms = int(p.num_matsubara_terms)
     d.truncation_level = int(p.hierarchy_truncation_level)
@@ -275,6 +284,15 @@ class Hierarchy:
         out = np.zeros(2 * self.n * self.n, np.float64)
         self._check(self.lib.phi_gpu_get_hamiltonian(self.ctx, out.ctypes.data))
         return from_col_major(out, self.n)
+
+    def rho0_full(self) -> np.ndarray:
+        """rho_0 in the full Hilbert space (V rho_0 V^+ under Hilbert-space
+        truncation; rho0() otherwise), F x F complex."""
+        F = ctypes.c_int32()
+        self._check(self.lib.phi_gpu_hilbert_space_size(self.ctx, ctypes.byref(F)))
+        out = np.zeros(2 * F.value * F.value, np.float64)
+        self._check(self.lib.phi_gpu_get_rho0_full(self.ctx, out.ctypes.data))
+        return from_col_major(out, F.value)
 
     def rho0(self) -> np.ndarray:
         out = np.zeros(2 * self.n * self.n, np.float64)

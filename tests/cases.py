@@ -150,3 +150,30 @@ def annealed(p: PhiParameters, t_end: float, seed: int = 0, samples: int = 5, co
     p.integration_time = t_end
     p.minimum_field_change = min_field_change
     return p
+
+
+def truncated_problem(full: int = 4, k: int = 3, baths: int = 2, matsubara: int = 2, truncation: int = 3,
+                      seed: int = 0, time_local: bool = False) -> PhiParameters:
+    """Hilbert-space truncated problem (PHI's HilbertSpaceSize > NumStates):
+    a real symmetric full x full Hamiltonian whose lowest k eigenvalues sit
+    apart from the rest, full bath coupling operators (real symmetric), a
+    full-space initial density matrix; the hierarchy keeps the lowest k
+    eigenvectors."""
+    rng = np.random.default_rng(seed)
+    Q, _ = np.linalg.qr(rng.normal(size=(full, full)))
+    e = np.concatenate([np.sort(rng.uniform(-60.0, 60.0, size=k)), np.sort(rng.uniform(250.0, 400.0, size=full - k))])
+    H = (Q * e) @ Q.T
+    H = (H + H.T) / 2
+    V = rng.normal(size=(baths, full, full))
+    V = (V + np.transpose(V, (0, 2, 1))) / 2
+    A = rng.normal(size=(full, full)) + 1j * rng.normal(size=(full, full))
+    rho = A @ np.conj(A.T)
+    rho /= np.trace(rho).real
+    p = PhiParameters(num_states=k, time_indepenent_hamiltonian=np.asarray(H, np.complex128),
+                      num_bath_couplings=baths, num_matsubara_terms=matsubara, hierarchy_truncation_level=truncation,
+                      temperature=300.0, is_full_bath_coupling=True, bath_coupling_op=V,
+                      initial_density_matrix=rho, hilbert_space_size=full)
+    p.gamma = rng.uniform(5.0, 20.0, size=baths)
+    p.lambda_ = rng.uniform(10.0, 40.0, size=baths)
+    p.use_time_local_truncation = time_local
+    return p

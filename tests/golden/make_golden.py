@@ -461,6 +461,39 @@ def make_fullsize_fixture(only=None):
         print(f"{cid}: {steps} steps ({accepted} accepted), {secs:.1f} s", flush=True)
 
 
+# Hilbert-space truncation, run by the reference built in BLAS mode (its
+# -DNOBLAS loops flip signs in the truncator): (case id, truncated_problem
+# kwargs, method, timestep, t_end).
+TRUNCATION_CASES = [
+    ("trunc_f4_k3_b2_k2_t3/rk4", dict(full=4, k=3, baths=2, matsubara=2, truncation=3, seed=1), "rk4", 0.001, 0.05),
+    ("trunc_f4_k3_b2_k2_t3/rkf45", dict(full=4, k=3, baths=2, matsubara=2, truncation=3, seed=1), "rkf45", 0.001,
+     0.05),
+    ("trunc_f5_k2_b3_k1_t3/rk4", dict(full=5, k=2, baths=3, matsubara=1, truncation=3, seed=2), "rk4", 0.001, 0.05),
+    ("trunc_f3_k2_vacuum/rk4", dict(full=3, k=2, baths=1, matsubara=1, truncation=1, seed=3), "rk4", 0.001, 0.05),
+    ("trunc_f4_k3_timelocal/rkf45", dict(full=4, k=3, baths=2, matsubara=2, truncation=3, seed=4, time_local=True),
+     "rkf45", 0.001, 0.05),
+]
+
+
+def make_truncation_fixture():
+    """ref_truncation.json: rho_0 (F x F, %.17g) of the BLAS-mode reference
+    build for Hilbert-space truncated problems."""
+    if not os.path.exists(O.REF_DRIVER_BLAS):
+        raise SystemExit("build the BLAS-mode reference first: make -C oracle/refbuild blas REF_SRC=... BLAS_LIB=...")
+    outs = []
+    for cid, kw, method, dt, t_end in TRUNCATION_CASES:
+        p = cases.truncated_problem(**kw)
+        if method == "rkf45":
+            p.fix_incompatible_combinations("rkf45")
+        rho, secs = O.run_reference(p, method, 1, timeout=300, driver=O.REF_DRIVER_BLAS, timestep=dt, t_end=t_end)
+        outs.append({"id": cid, "kwargs": kw, "method": method, "timestep": dt, "t_end": t_end,
+                     "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]})
+        print(f"{cid}: {secs:.3f}s", flush=True)
+    with open(os.path.join(HERE, "ref_truncation.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py truncation (reference built in BLAS mode)",
+                   "cases": outs}, f, indent=0)
+
+
 def make_fullsize_decisions():
     """For each full-size RKF45 case of ref_fullsize.json: the oracle's error
     estimate of every attempted step and the accept decision it leads to
@@ -507,6 +540,9 @@ def main():
     if len(sys.argv) > 2 and sys.argv[2] == "fullsize":
         make_fullsize_fixture(sys.argv[3:] or None)
         make_fullsize_decisions()
+        return
+    if len(sys.argv) > 2 and sys.argv[2] == "truncation":
+        make_truncation_fixture()
         return
     if len(sys.argv) > 2 and sys.argv[2] == "fullsize_decisions":
         make_fullsize_decisions()
