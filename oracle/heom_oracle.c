@@ -52,6 +52,12 @@ struct oracle_ctx {
   struct spline { int n, last; double *x, *a, *b, *c, *d; } sx, sz;
   double old_fx, old_fz;          /* old_*_field_value_th_ */
   double integration_time, min_field_change;
+  /* Hilbert-space truncation of the annealing Hamiltonian: F > N, hx / hz
+   * are F x F, V the current basis (F x N, real, column-major), V0 and
+   * bath0 the initial basis and truncated bath operators. */
+  int F;
+  double *V, *V0;
+  cplx *bath0;
 };
 
 /* ------------------------------------------------------------------------ */
@@ -235,18 +241,183 @@ void oracle_get_hamiltonian(const oracle_ctx *c, double *h) {
   memcpy(h, c->H, sizeof(cplx) * (size_t)(c->N * c->N));
 }
 
+static void fill_full_bath_tables(oracle_ctx *c);
+static void truncate_op(int F, int k, const double *V, const cplx *A, cplx *to);
+
 void oracle_reset_hamiltonian(oracle_ctx *c) {
   if (!c->anneal) return;
   const int E = c->N * c->N;
   for (int k = 0; k < E; ++k) c->H[k] = c->Hadj[k] = 0;
   c->old_fx = c->old_fz = DBL_MAX;   /* numeric_limits<Float>::max() (:518-523) */
   c->sx.last = c->sz.last = 0;
+  if (c->F > c->N) {
+    memcpy(c->V, c->V0, sizeof(double) * (size_t)c->F * c->N);
+    if (c->bath0) {
+      memcpy(c->bath, c->bath0, sizeof(cplx) * (size_t)(c->nb * E));
+      fill_full_bath_tables(c);
+    }
+  }
 }
 
-/* UpdateTimeDependentHamiltonian (hierarchy_integrator.cc:1618-1673), no
- * Hilbert-space truncation: H = f_x H_X + f_z H_Z at alpha = t / T, applied
- * only when either field moved by at least the minimum relative change. */
-static void anneal_update(const oracle_ctx *cc, double time) {
+int oracle_hilbert_space_size(const oracle_ctx *c) { return c->F > c->N ? c->F : c->N; }
+
+void oracle_truncate(const oracle_ctx *c, const double *full, double *out) {
+  const int F = c->F;
+  cplx *a = (cplx *)malloc(sizeof(cplx) * (size_t)F * F);
+  for (int k = 0; k < F * F; ++k) a[k] = cx(full[2 * k], full[2 * k + 1]);
+  truncate_op(F, c->N, c->V0, a, (cplx *)out);
+  free(a);
+}
+
+void oracle_get_basis(const oracle_ctx *c, double *basis) {
+  memcpy(basis, c->V, sizeof(double) * (size_t)c->F * c->N);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Hilbert-space truncation of an annealing Hamiltonian.                     */
+
+/* Eigenvalues (ascending) and orthonormal eigenvectors of a real symmetric
+ * n x n matrix by the cyclic Jacobi method (Jacobi 1846; rotations as in
+ * Rutishauser's formulation): a (column-major) is overwritten, w gets the
+ * eigenvalues, v (n x n) the eigenvectors in the same order.  Stands in for
+ * LAPACK's zheevr (lapack_wrapper.h:71-96); the kept subspace does not depend
+ * on the method when eigenvalues k and k+1 are apart. */
+static void jacobi_sym(int n, double *a, double *w, double *v) {
+  for (int i = 0; i < n * n; ++i) v[i] = 0;
+  for (int i = 0; i < n; ++i) v[i + i * n] = 1;
+  double scale = 0;
+  for (int i = 0; i < n * n; ++i) scale = fmax(scale, fabs(a[i]));
+  for (int sweep = 0; sweep < 100 && scale > 0; ++sweep) {
+    double off = 0;
+    for (int q = 0; q < n; ++q)
+      for (int p = 0; p < q; ++p) off += a[p + q * n] * a[p + q * n];
+    if (sqrt(off) <= 1e-16 * scale) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        const double apq = a[p + q * n];
+        if (fabs(apq) <= 1e-300) continue;
+        const double th = (a[q + q * n] - a[p + p * n]) / (2 * apq);
+        const double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+        const double cs = 1 / sqrt(t * t + 1), sn = t * cs;
+        for (int r = 0; r < n; ++r) {
+          const double x = a[r + p * n], y = a[r + q * n];
+          a[r + p * n] = cs * x - sn * y;
+          a[r + q * n] = sn * x + cs * y;
+        }
+        for (int r = 0; r < n; ++r) {
+          const double x = a[p + r * n], y = a[q + r * n];
+          a[p + r * n] = cs * x - sn * y;
+          a[q + r * n] = sn * x + cs * y;
+        }
+        a[p + q * n] = a[q + p * n] = 0;
+        for (int r = 0; r < n; ++r) {
+          const double x = v[r + p * n], y = v[r + q * n];
+          v[r + p * n] = cs * x - sn * y;
+          v[r + q * n] = sn * x + cs * y;
+        }
+      }
+  }
+  /* Selection sort of the eigenpairs by eigenvalue (stable for ties). */
+  for (int i = 0; i < n; ++i) w[i] = a[i + i * n];
+  for (int i = 0; i < n; ++i) {
+    int best = i;
+    for (int j = i + 1; j < n; ++j)
+      if (w[j] < w[best]) best = j;
+    if (best != i) {
+      const double tw = w[i];
+      w[i] = w[best];
+      w[best] = tw;
+      for (int r = 0; r < n; ++r) {
+        const double tv = v[r + i * n];
+        v[r + i * n] = v[r + best * n];
+        v[r + best * n] = tv;
+      }
+    }
+  }
+}
+
+/* The lowest k eigenvectors of the real part of the F x F matrix h (F x k,
+ * column-major, into out).  With a previous basis, each kept vector takes
+ * the sign that makes its overlap with the previous vector of the same index
+ * non-negative (LAPACK's signs are arbitrary; any choice gives the same
+ * truncated dynamics, and this one keeps the rotation near the identity). */
+static void lowest_eigenvectors(int F, int k, const cplx *h, const double *prev, double *out) {
+  double *a = (double *)malloc(sizeof(double) * (size_t)F * F);
+  double *w = (double *)malloc(sizeof(double) * (size_t)F);
+  double *v = (double *)malloc(sizeof(double) * (size_t)F * F);
+  for (int i = 0; i < F * F; ++i) a[i] = creal(h[i]);
+  jacobi_sym(F, a, w, v);
+  for (int j = 0; j < k; ++j) {
+    double d = 0;
+    if (prev)
+      for (int r = 0; r < F; ++r) d += prev[r + j * F] * v[r + j * F];
+    const double sg = d < 0 ? -1.0 : 1.0;
+    for (int r = 0; r < F; ++r) out[r + j * F] = sg * v[r + j * F];
+  }
+  free(a); free(w); free(v);
+}
+
+/* HilbertSpaceTruncator::Truncate (hilbert_space_truncator.cc:34-58) with a
+ * real basis: to(j, i) = v_j^T A v_i for j <= i, to(i, j) its conjugate. */
+static void truncate_op(int F, int k, const double *V, const cplx *A, cplx *to) {
+  cplx *work = (cplx *)malloc(sizeof(cplx) * (size_t)F);
+  for (int i = 0; i < k; ++i) {
+    for (int r = 0; r < F; ++r) {
+      cplx acc = 0;
+      for (int l = 0; l < F; ++l) acc += A[r + l * F] * V[l + i * F];
+      work[r] = acc;
+    }
+    for (int j = 0; j <= i; ++j) {
+      cplx acc = 0;
+      for (int r = 0; r < F; ++r) acc += V[r + j * F] * work[r];
+      to[j + i * k] = acc;
+      to[i + j * k] = conj(acc);
+    }
+  }
+  free(work);
+}
+
+/* HilbertSpaceTruncator::Rotate (:63-74) in BLAS mode: zhemm reads A as
+ * Hermitian from its upper triangle (diagonal real), so A <- R herm(A) R^+,
+ * R(j, i) = <old_i | new_j> (:104-112). */
+static void rotate_op(int k, const double *R, cplx *A, cplx *work) {
+  for (int j = 0; j < k; ++j)    /* work = herm(A) R^T */
+    for (int i = 0; i < k; ++i) {
+      cplx acc = 0;
+      for (int b = 0; b < k; ++b) {
+        const cplx ab = i < b ? A[i + b * k] : (i > b ? conj(A[b + i * k]) : creal(A[i + i * k]));
+        acc += ab * R[j + b * k];
+      }
+      work[i + j * k] = acc;
+    }
+  for (int j = 0; j < k; ++j)    /* A = R work */
+    for (int i = 0; i < k; ++i) {
+      cplx acc = 0;
+      for (int a = 0; a < k; ++a) acc += R[i + a * k] * work[a + j * k];
+      A[i + j * k] = acc;
+    }
+}
+
+/* Hierarchy::FillFullBathOperators (hierarchy.cc:203-216). */
+static void fill_full_bath_tables(oracle_ctx *c) {
+  const int E = c->N * c->N;
+  for (int m = 0; m < c->nb; ++m)
+    for (int k = 0; k < E; ++k) {
+      c->same[m * E + k] = csqrt(c->matsubara[m]) * c->bath[m * E + k];
+      c->nextop[m * E + k] = cx(0, -1) * c->bath[m * E + k];
+      c->prevop[m * E + k] = -c->bath[m * E + k];
+    }
+}
+
+/* UpdateTimeDependentHamiltonian (hierarchy_integrator.cc:1618-1673):
+ * H = f_x H_X + f_z H_Z at alpha = t / T, applied only when either field
+ * moved by at least the minimum relative change.  With Hilbert-space
+ * truncation the full H is re-diagonalised (UpdateWith, :101-113), H is
+ * truncated into the new basis, the bath operators are rotated when the
+ * hierarchy has more than one tier or time-local truncation (:1661-1668),
+ * and the caller's live ADO arrays (live[0..nlive), M*N*N each) are rotated
+ * (:1990-1995 and the other stage times) -- the time-local matrices are not. */
+static void anneal_update(const oracle_ctx *cc, double time, cplx *const *live, int nlive) {
   oracle_ctx *c = (oracle_ctx *)cc;
   if (!c->anneal) return;
   const double alpha = time / c->integration_time;
@@ -257,7 +428,32 @@ static void anneal_update(const oracle_ctx *cc, double time) {
   c->old_fx = creal(fx);
   c->old_fz = creal(fz);
   const int N = c->N;
-  for (int k = 0; k < N * N; ++k) c->H[k] = fx * c->hx[k] + fz * c->hz[k];
+  if (c->F > N) {
+    const int F = c->F, E = N * N;
+    cplx *hf = (cplx *)malloc(sizeof(cplx) * (size_t)F * F);
+    for (int k = 0; k < F * F; ++k) hf[k] = fx * c->hx[k] + fz * c->hz[k];
+    double *vn = (double *)malloc(sizeof(double) * (size_t)F * N);
+    lowest_eigenvectors(F, N, hf, c->V, vn);
+    double *R = (double *)malloc(sizeof(double) * (size_t)E);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double d = 0;
+        for (int r = 0; r < F; ++r) d += c->V[r + i * F] * vn[r + j * F];
+        R[j + i * N] = d;
+      }
+    memcpy(c->V, vn, sizeof(double) * (size_t)F * N);
+    truncate_op(F, N, c->V, hf, c->H);
+    cplx *work = (cplx *)malloc(sizeof(cplx) * (size_t)E);
+    if (c->kind == ORACLE_BATH_FULL && (c->trunc > 1 || c->tl)) {
+      for (int m = 0; m < c->nb; ++m) rotate_op(N, R, c->bath + (size_t)m * E, work);
+      fill_full_bath_tables(c);
+    }
+    for (int v = 0; v < nlive; ++v)
+      for (int64_t m = 0; m < c->M; ++m) rotate_op(N, R, live[v] + m * E, work);
+    free(hf); free(vn); free(R); free(work);
+  } else {
+    for (int k = 0; k < N * N; ++k) c->H[k] = fx * c->hx[k] + fz * c->hz[k];
+  }
   for (int r = 0; r < N; ++r)
     for (int col = 0; col < N; ++col) c->Hadj[r + col * N] = conj(c->H[col + r * N]);
 }
@@ -330,13 +526,16 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
 
   c->H = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
   c->Hadj = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
+  double *trunc_coupling = NULL;
   if (p->h_x) {
     /* Annealing: the Hamiltonian stays zero until the first update
      * (hierarchy_integrator.cc:891-944 copies no static H). */
     c->anneal = 1;
-    c->hx = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
-    c->hz = (cplx *)malloc(sizeof(cplx) * (size_t)(N * N));
-    for (int k = 0; k < N * N; ++k) {
+    const int F = p->hilbert_space_size > N ? p->hilbert_space_size : N;
+    c->F = F;
+    c->hx = (cplx *)malloc(sizeof(cplx) * (size_t)(F * F));
+    c->hz = (cplx *)malloc(sizeof(cplx) * (size_t)(F * F));
+    for (int k = 0; k < F * F; ++k) {
       c->hx[k] = cx(p->h_x[2 * k], p->h_x[2 * k + 1]);
       c->hz[k] = cx(p->h_z[2 * k], p->h_z[2 * k + 1]);
     }
@@ -344,7 +543,30 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
     spline_init(&c->sz, p->field_z, p->num_field_z);
     c->integration_time = p->integration_time;
     c->min_field_change = p->min_field_change;
-    oracle_reset_hamiltonian(c);
+    if (F > N) {
+      /* The truncator is first updated with H at alpha = 0 (:934-946); the
+       * initial density matrix and full bath operators are truncated into
+       * that basis (:1073-1075, :1179-1186). */
+      const cplx f0x = spline_get(&c->sx, 0.0), f0z = spline_get(&c->sz, 0.0);
+      cplx *h0 = (cplx *)malloc(sizeof(cplx) * (size_t)F * F);
+      for (int k = 0; k < F * F; ++k) h0[k] = f0x * c->hx[k] + f0z * c->hz[k];
+      c->V = (double *)malloc(sizeof(double) * (size_t)F * N);
+      c->V0 = (double *)malloc(sizeof(double) * (size_t)F * N);
+      lowest_eigenvectors(F, N, h0, NULL, c->V0);
+      free(h0);
+      if (p->bath_kind == ORACLE_BATH_FULL && p->coupling) {
+        const size_t E = (size_t)N * N;
+        trunc_coupling = (double *)malloc(sizeof(double) * (size_t)p->num_baths * E);
+        cplx *full = (cplx *)malloc(sizeof(cplx) * (size_t)F * F);
+        cplx *tk = (cplx *)malloc(sizeof(cplx) * E);
+        for (int m = 0; m < p->num_baths; ++m) {
+          for (int k = 0; k < F * F; ++k) full[k] = cx(p->coupling[(size_t)m * F * F + k], 0);
+          truncate_op(F, N, c->V0, full, tk);
+          for (size_t k = 0; k < E; ++k) trunc_coupling[m * E + k] = creal(tk[k]);
+        }
+        free(full); free(tk);
+      }
+    }
   } else {
     for (int k = 0; k < N * N; ++k) c->H[k] = cx(p->hamiltonian[2 * k], p->hamiltonian[2 * k + 1]);
     for (int r = 0; r < N; ++r)  /* ConjugateTranspose (complex_matrix.cc) */
@@ -414,18 +636,20 @@ oracle_ctx *oracle_create(const oracle_problem *p) {
     }
   } else if (c->kind == ORACLE_BATH_FULL) {
     /* Hierarchy::FillFullBathOperators (hierarchy.cc:203-216). */
+    const double *cp = trunc_coupling ? trunc_coupling : p->coupling;
     c->bath = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
-    for (int k = 0; k < c->nb * E; ++k) c->bath[k] = cx(p->coupling[k], 0);
+    for (int k = 0; k < c->nb * E; ++k) c->bath[k] = cx(cp[k], 0);
     c->same = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
     c->nextop = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
     c->prevop = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
-    for (int m = 0; m < c->nb; ++m)
-      for (int k = 0; k < E; ++k) {
-        c->same[m * E + k] = csqrt(c->matsubara[m]) * c->bath[m * E + k];
-        c->nextop[m * E + k] = cx(0, -1) * c->bath[m * E + k];
-        c->prevop[m * E + k] = -c->bath[m * E + k];
-      }
+    fill_full_bath_tables(c);
+    if (c->F > N) {
+      c->bath0 = (cplx *)malloc(sizeof(cplx) * (size_t)(c->nb * E));
+      memcpy(c->bath0, c->bath, sizeof(cplx) * (size_t)(c->nb * E));
+    }
   }
+  free(trunc_coupling);
+  if (c->anneal) oracle_reset_hamiltonian(c);
   return c;
 }
 
@@ -435,7 +659,7 @@ void oracle_destroy(oracle_ctx *c) {
   free(c->H); free(c->Hadj); free(c->corr); free(c->abs_corr); free(c->matsubara); free(c->gamma);
   free(c->bath); free(c->same); free(c->nextop); free(c->prevop); free(c->active);
   free(c->tlqk); free(c->tlqk_st); free(c->tlq); free(c->tlq_st); free(c->tlqa);
-  free(c->hx); free(c->hz);
+  free(c->hx); free(c->hz); free(c->V); free(c->V0); free(c->bath0);
   free(c->sx.x); free(c->sx.a); free(c->sx.b); free(c->sx.c); free(c->sx.d);
   free(c->sz.x); free(c->sz.a); free(c->sz.b); free(c->sz.c); free(c->sz.d);
   free(c);
@@ -888,17 +1112,26 @@ int64_t oracle_rk4(const oracle_ctx *c, double *state_d, double dt, double start
   int64_t i = -1, nout = 0;
   while (time_now < end_time) {
     i += 1;
-    anneal_update(c, time_now);                                   /* :2688 */
+    {
+      cplx *live[] = {y};
+      anneal_update(c, time_now, live, 1);                        /* :2688-2695 */
+    }
     apply_all(c, y, k0, temp);                                   /* :2709-2711 */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k0[j] * h2; /* :2715-2718 */
     tl_update(c, dt / 2);                                         /* :2721 */
-    anneal_update(c, time_now + dt / 2);                          /* :2728 */
+    {
+      cplx *live[] = {y, x, k0};
+      anneal_update(c, time_now + dt / 2, live, 3);               /* :2728-2737 */
+    }
     apply_all(c, x, k1, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k1[j] * h2; /* :2758-2761 */
     apply_all(c, x, k2, temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k2[j] * h1; /* :2777-2780 */
     tl_update(c, dt / 2);                                         /* :2784 */
-    anneal_update(c, time_now + dt);                              /* :2792 */
+    {
+      cplx *live[] = {y, x, k0, k1, k2};
+      anneal_update(c, time_now + dt, live, 5);                   /* :2792-2803 */
+    }
     apply_all(c, x, k3, temp);
     for (int64_t j = 0; j < total; ++j)                           /* :2822-2825 */
       y[j] += h6 * (k0[j] + 2.0 * k1[j] + 2.0 * k2[j] + k3[j]);
@@ -961,35 +1194,54 @@ int64_t oracle_rkf45_trace(const oracle_ctx *c, double *state_d, double dt0, dou
   int64_t i = -1, accepted = 0;
   while (time_now < end_time) {
     i += 1;
-    anneal_update(c, time_now);                                   /* :1988 */
+    {
+      cplx *live[] = {y};
+      anneal_update(c, time_now, live, 1);                        /* :1988-1995 */
+    }
     apply_all(c, y, k[0], temp);
     /* Time-local matrices and an annealing Hamiltonian follow the stage
      * times (:1988, :2028-2033, :2079-2084, :2132-2138, :2188-2194,
      * :2246-2252). */
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b10;
     tl_update(c, a[0]);
-    anneal_update(c, time_now + a[0]);
+    {
+      cplx *live[] = {y, x, k[0]};
+      anneal_update(c, time_now + a[0], live, 3);
+    }
     apply_all(c, x, k[1], temp);
     for (int64_t j = 0; j < total; ++j) x[j] = y[j] + k[0][j] * b20 + k[1][j] * b21;
     tl_update(c, a[1] - a[0]);
-    anneal_update(c, time_now + a[1]);
+    {
+      cplx *live[] = {y, x, k[0], k[1]};
+      anneal_update(c, time_now + a[1], live, 4);
+    }
     apply_all(c, x, k[2], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b30 + k[1][j] * b31 + k[2][j] * b32;
     tl_update(c, a[2] - a[1]);
-    anneal_update(c, time_now + a[2]);
+    {
+      cplx *live[] = {y, x, k[0], k[1], k[2]};
+      anneal_update(c, time_now + a[2], live, 5);
+    }
     apply_all(c, x, k[3], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b40 + k[1][j] * b41 + k[2][j] * b42 + k[3][j] * b43;
     tl_update(c, a[3] - a[2]);
-    anneal_update(c, time_now + a[3]);
+    {
+      cplx *live[] = {y, x, k[0], k[1], k[2], k[3]};
+      anneal_update(c, time_now + a[3], live, 6);
+    }
     apply_all(c, x, k[4], temp);
     for (int64_t j = 0; j < total; ++j)
       x[j] = y[j] + k[0][j] * b50 + k[1][j] * b51 + k[2][j] * b52 + k[3][j] * b53 +
              k[4][j] * b54;
     tl_restore(c);
     tl_update(c, a[4]);
-    anneal_update(c, time_now + a[4]);
+    {
+      /* k1 is not rotated at this stage (:2259-2263): no later sum reads it. */
+      cplx *live[] = {y, x, k[0], k[2], k[3], k[4]};
+      anneal_update(c, time_now + a[4], live, 6);
+    }
     apply_all(c, x, k[5], temp);
     /* Fourth- and fifth-order solutions and the global max-abs difference
      * (:2317-2328, :2339-2351); x holds the fifth-order candidate. */

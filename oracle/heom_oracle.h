@@ -54,6 +54,12 @@ typedef struct {
   int num_field_x, num_field_z;   /* >= 2 each */
   double integration_time;        /* T (PhiParameters::integration_time) */
   double min_field_change;        /* PhiParameters::minimum_field_change */
+  /* Hilbert-space truncation of an annealing Hamiltonian
+   * (PhiParameters::hilbert_space_size F > num_states = k): h_x, h_z and full
+   * coupling operators are F x F, real; the hierarchy runs in the lowest k
+   * eigenvectors of H(t), re-diagonalised at every Hamiltonian update.
+   * 0 or num_states: no truncation. */
+  int hilbert_space_size;
 } oracle_problem;
 
 typedef struct oracle_ctx oracle_ctx;
@@ -102,6 +108,16 @@ void oracle_reset_hamiltonian(oracle_ctx *c);
 void oracle_get_hamiltonian(const oracle_ctx *c, double *h);
 void oracle_get_time_local(const oracle_ctx *c, double *q);
 void oracle_get_active(const oracle_ctx *c, unsigned char *flags);
+
+/* Truncated annealing contexts: Truncate (hilbert_space_truncator.cc:34-58)
+ * of a full F x F operator into the initial basis (the lowest k eigenvectors
+ * of H(0)), written as 2*k*k doubles; and the current basis V (F x k real,
+ * column-major), which the Hamiltonian updates rotate.  rho_0 in the full
+ * space is V rho_0 V^T (UnTruncate, :76-88).  oracle_reset_hamiltonian puts
+ * the basis and the bath operators back to their initial values. */
+int oracle_hilbert_space_size(const oracle_ctx *c);
+void oracle_truncate(const oracle_ctx *c, const double *full, double *out);
+void oracle_get_basis(const oracle_ctx *c, double *basis);
 
 /* Initial hierarchy state: rho(0) scaled into node 0, zeros elsewhere
  * (hierarchy_integrator.cc:1070-1096). */

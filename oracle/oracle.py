@@ -41,6 +41,7 @@ class _Problem(ctypes.Structure):
         ("field_x", POINTER(c_double)), ("field_z", POINTER(c_double)),
         ("num_field_x", c_int), ("num_field_z", c_int),
         ("integration_time", c_double), ("min_field_change", c_double),
+        ("hilbert_space_size", c_int),
     ]
 
 
@@ -84,6 +85,10 @@ def load():
                                  c_double, POINTER(c_int64), POINTER(c_double), POINTER(c_double)]
     lib.oracle_set_threads.restype = None
     lib.oracle_set_threads.argtypes = [ctypes.c_int]
+    lib.oracle_hilbert_space_size.restype = c_int
+    lib.oracle_hilbert_space_size.argtypes = [c_void_p]
+    lib.oracle_truncate.argtypes = [c_void_p, c_void_p, c_void_p]
+    lib.oracle_get_basis.argtypes = [c_void_p, c_void_p]
     lib.oracle_rkf45_trace.restype = c_int64
     lib.oracle_rkf45_trace.argtypes = [c_void_p, c_void_p, c_double, c_double, c_double, c_double,
                                        c_double, POINTER(c_int64), POINTER(c_double), POINTER(c_double),
@@ -141,6 +146,13 @@ class Oracle:
 
         pr = _Problem()
         pr.num_states = n
+        # Hilbert-space truncation of an annealing Hamiltonian: operators are
+        # F x F; the oracle keeps the basis (static truncation is restated in
+        # the tests on the projected problem).
+        hs = int(getattr(p, "hilbert_space_size", 0) or 0)
+        annealing = getattr(p, "transverse_hamiltonian", None) is not None
+        F = hs if (annealing and hs > n) else n
+        self.F = F
         pr.num_baths = int(p.num_bath_couplings)
         pr.num_matsubara = int(p.num_matsubara_terms)
         pr.truncation = int(p.hierarchy_truncation_level)
@@ -156,7 +168,7 @@ class Oracle:
         if pr.bath_kind == 1:
             pr.coupling = arr(np.asarray(p.bath_coupling_op, np.float64))
         elif pr.bath_kind == 2:
-            v = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, n, n)
+            v = np.asarray(p.bath_coupling_op, np.float64).reshape(-1, F, F)
             pr.coupling = arr(np.transpose(v, (0, 2, 1)))
         # FixIncompatibleCombinations (phi_parameters.cc:847-851): filtering
         # only with independent baths.
@@ -174,6 +186,7 @@ class Oracle:
             pr.num_field_x, pr.num_field_z = fx.size, fz.size
             pr.integration_time = float(p.integration_time)
             pr.min_field_change = float(p.minimum_field_change)
+            pr.hilbert_space_size = F
         self._keep = keep
         self.ctx = self.lib.oracle_create(ctypes.byref(pr))
         if not self.ctx:
@@ -181,6 +194,10 @@ class Oracle:
         self.M = int(self.lib.oracle_num_nodes(self.ctx))
         self.T = int(self.lib.oracle_num_terms(self.ctx))
         self.rho_init = _colmajor(p.initial_density_matrix)
+        if F > n:
+            out = np.zeros(2 * n * n)
+            self.lib.oracle_truncate(self.ctx, self.rho_init.ctypes.data, out.ctypes.data)
+            self.rho_init = out
 
     def __del__(self):
         if getattr(self, "ctx", None):
@@ -290,6 +307,21 @@ class Oracle:
 
     def rho0(self, state):
         return _from_colmajor(np.asarray(state)[:2 * self.n * self.n], self.n)
+
+    def basis(self):
+        """Current truncation basis V (F x N real) of a truncated annealing
+        run; the identity without truncation."""
+        if self.F == self.n:
+            return np.eye(self.n)
+        v = np.zeros(self.F * self.n)
+        self.lib.oracle_get_basis(self.ctx, v.ctypes.data)
+        return v.reshape(self.n, self.F).T
+
+    def rho0_full(self, state):
+        """rho_0 in the full Hilbert space, V rho_0 V^T (UnTruncate,
+        hilbert_space_truncator.cc:76-88), after the last run."""
+        V = self.basis()
+        return V @ self.rho0(state) @ V.T
 
     # -- steady state --------------------------------------------------------
     # Coordinates of a Hermitian ADO X (N*N reals, in the column-major element

@@ -55,6 +55,12 @@ Outputs (committed; the GPU host has no reference tree):
 
     python tests/golden/make_golden.py /root/reference anneal    # annealing fixture only
     python tests/golden/make_golden.py /root/reference restart_tl # time-local restart fixture only
+  ref_trunc_anneal.json Hilbert-space truncation of annealing Hamiltonians,
+                        rho_0 (F x F, %.17g) from the reference built in BLAS
+                        mode (oracle/_ref_blas): seeded problems and the
+                        problems of the reference's truncated annealing tests
+
+    python tests/golden/make_golden.py /root/reference trunc_anneal
 """
 from __future__ import annotations
 
@@ -494,6 +500,55 @@ def make_truncation_fixture():
                    "cases": outs}, f, indent=0)
 
 
+# (case id, builder, kwargs, method, timestep, t_end): Hilbert-space truncation
+# of annealing Hamiltonians.  "truncated_annealed" draws seeded problems;
+# "reference_truncated_anneal" builds the problems of the reference's own
+# truncated annealing tests.
+TRUNC_ANNEAL_CASES = [
+    ("ta_f4_k2_t3/rkf45", "truncated_annealed", dict(full=4, k=2, seed=1), "rkf45", 0.001, 0.05),
+    ("ta_f4_k2_t3/rk4", "truncated_annealed", dict(full=4, k=2, seed=1), "rk4", 0.001, 0.05),
+    ("ta_f5_k3_t2/rk4", "truncated_annealed", dict(full=5, k=3, seed=2, truncation=2), "rk4", 0.001, 0.05),
+    ("ta_f4_k3_t1/rkf45", "truncated_annealed", dict(full=4, k=3, seed=4, truncation=1), "rkf45", 0.001, 0.05),
+    ("ta_f4_k2_t3_gate0.2/rkf45", "truncated_annealed", dict(full=4, k=2, seed=5, min_field_change=0.2), "rkf45",
+     0.001, 0.05),
+    ("ta_f4_k2_t3_timelocal/rkf45", "truncated_annealed", dict(full=4, k=2, seed=3, time_local=True), "rkf45",
+     0.001, 0.05),
+    ("refcfg_vacuum/rk4", "reference_truncated_anneal", dict(test="vacuum"), "rk4", 0.001, 1.0),
+    ("refcfg_vacuum/rkf45", "reference_truncated_anneal", dict(test="vacuum"), "rkf45", 0.001, 1.0),
+    ("refcfg_medium_full_indep/rk4", "reference_truncated_anneal", dict(test="medium_full_indep"), "rk4", 0.001,
+     1.0),
+    ("refcfg_medium_full_indep/rkf45", "reference_truncated_anneal", dict(test="medium_full_indep"), "rkf45",
+     0.001, 1.0),
+    ("refcfg_weak_full_indep_tl/rkf45", "reference_truncated_anneal", dict(test="weak_full_indep_tl"), "rkf45",
+     0.001, 10.0),
+    ("refcfg_weak_full_tl/rkf45", "reference_truncated_anneal", dict(test="weak_full_tl"), "rkf45", 0.001, 10.0),
+]
+
+
+def trunc_anneal_problem(builder, kw, method):
+    p = getattr(cases, builder)(**kw)
+    if method == "rkf45":
+        p.fix_incompatible_combinations("rkf45")
+    return p
+
+
+def make_trunc_anneal_fixture():
+    """ref_trunc_anneal.json: rho_0 (F x F, %.17g) of the BLAS-mode reference
+    build for Hilbert-space truncated annealing problems."""
+    if not os.path.exists(O.REF_DRIVER_BLAS):
+        raise SystemExit("build the BLAS-mode reference first: make -C oracle/refbuild blas REF_SRC=... BLAS_LIB=...")
+    outs = []
+    for cid, builder, kw, method, dt, t_end in TRUNC_ANNEAL_CASES:
+        p = trunc_anneal_problem(builder, kw, method)
+        rho, secs = O.run_reference(p, method, 1, timeout=600, driver=O.REF_DRIVER_BLAS, timestep=dt, t_end=t_end)
+        outs.append({"id": cid, "builder": builder, "kwargs": kw, "method": method, "timestep": dt, "t_end": t_end,
+                     "rho0_colmajor": [[float(z.real), float(z.imag)] for z in rho.T.reshape(-1)]})
+        print(f"{cid}: {secs:.3f}s", flush=True)
+    with open(os.path.join(HERE, "ref_trunc_anneal.json"), "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py trunc_anneal (reference built in BLAS mode)",
+                   "cases": outs}, f, indent=0)
+
+
 def make_fullsize_decisions():
     """For each full-size RKF45 case of ref_fullsize.json: the oracle's error
     estimate of every attempted step and the accept decision it leads to
@@ -543,6 +598,9 @@ def main():
         return
     if len(sys.argv) > 2 and sys.argv[2] == "truncation":
         make_truncation_fixture()
+        return
+    if len(sys.argv) > 2 and sys.argv[2] == "trunc_anneal":
+        make_trunc_anneal_fixture()
         return
     if len(sys.argv) > 2 and sys.argv[2] == "fullsize_decisions":
         make_fullsize_decisions()

@@ -1,0 +1,95 @@
+"""Hilbert-space truncation of an annealing Hamiltonian, CPU side: the
+oracle against rho_0 (%.17g) of the reference built in BLAS mode
+(tests/golden/ref_trunc_anneal.json) and against the solutions hard-coded in
+the reference's own truncated annealing tests
+(src/hierarchy_integrator_test.cc:554-557, :582-585, :625-628, :690-698).
+
+PHI re-diagonalises the full Hamiltonian at every Hamiltonian update
+(hierarchy_integrator.cc:1618-1673), truncates H into the new basis, and
+rotates every live ADO and the bath operators from the old basis into the
+new one (hilbert_space_truncator.cc:63-74, :101-113).  Without time-local
+truncation the result does not depend on the signs LAPACK gives the
+eigenvectors, and the oracle (Jacobi eigenvectors, each signed to overlap
+its predecessor positively) matches the reference build to rounding.  With
+time-local truncation PHI does not rotate the Q matrices, so its result
+depends on those signs: LAPACK's zheevr flips the sign of an eigenvector from
+one update to the next even where the eigenbasis does not move.  Those cases
+are held to the reference's own RKF45 test tolerance, 1e-3 (measured:
+2.4e-4 and 2.8e-4 on the two affected fixtures)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from oracle import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+FIX = json.load(open(os.path.join(HERE, "golden", "ref_trunc_anneal.json")))["cases"]
+TOL = 1e-10
+TL_TOL = 1e-3  # assertMatrixSomewhatEqual (hierarchy_integrator_test.cc:289-306)
+
+
+def _rho(case):
+    v = np.array(case["rho0_colmajor"])
+    F = int(round(len(v) ** 0.5))
+    return (v[:, 0] + 1j * v[:, 1]).reshape(F, F).T
+
+
+def problem(case):
+    p = getattr(cases, case["builder"])(**case["kwargs"])
+    if case["method"] == "rkf45":
+        p.fix_incompatible_combinations("rkf45")
+    return p
+
+
+def run_oracle(case):
+    p = problem(case)
+    o = O.Oracle(p)
+    if case["method"] == "rk4":
+        s, *_ = o.rk4(o.initial_state(), case["timestep"], case["t_end"])
+    else:
+        s, _ = o.rkf45(o.initial_state(), case["timestep"], case["t_end"], p.rkf45_tolerance,
+                       p.rkf45_minimum_timestep)
+    return o.rho0_full(s), p
+
+
+@pytest.mark.parametrize("case", FIX, ids=[c["id"] for c in FIX])
+def test_oracle_matches_reference_build(case):
+    got, p = run_oracle(case)
+    tol = TL_TOL if p.use_time_local_truncation else TOL
+    assert np.abs(got - _rho(case)).max() <= tol
+
+
+# The reference tests' solutions (raw arrays, PHI's storage order) and their
+# tolerances: RK4 1e-6 (assertMatrixAlmostEqual), RKF45 1e-3.
+VACUUM = [0.777864, 0.315941 - 0.270135j, 0.315941 + 0.270135j, 0.222136]
+MEDIUM = [0.811767, 0.128111 - 0.144969j, 0.128111 + 0.144969j, 0.188233]
+WEAK_TL = [0.467201, 0.255327 + 0.207856j, 0.255327 - 0.207856j, 0.532799]
+WEAK_FULL_TL = [0.267895, -0.0281567 - 0.0246088j, -0.00247109 - 0.0184745j,
+                -0.0281567 + 0.0246088j, 0.208783, 0.154777 + 0.00171474j,
+                -0.00247109 + 0.0184745j, 0.154777 - 0.00171474j, 0.116023]
+
+
+def _embed(two):
+    m = np.zeros((3, 3), np.complex128)
+    m[:2, :2] = np.asarray(two).reshape(2, 2)
+    return m.reshape(-1)
+
+
+REF_TESTS = [("vacuum", "rk4", _embed(VACUUM), 1e-6), ("vacuum", "rkf45", _embed(VACUUM), 1e-3),
+             ("medium_full_indep", "rk4", _embed(MEDIUM), 1e-6),
+             ("medium_full_indep", "rkf45", _embed(MEDIUM), 1e-3),
+             ("weak_full_indep_tl", "rkf45", _embed(WEAK_TL), 1e-3),
+             ("weak_full_tl", "rkf45", np.asarray(WEAK_FULL_TL), 1e-3)]
+
+
+@pytest.mark.parametrize("test,method,expected,tol", REF_TESTS,
+                         ids=[f"{t}/{m}" for t, m, _, _ in REF_TESTS])
+def test_oracle_passes_reference_truncated_anneal_tests(test, method, expected, tol):
+    case = {"builder": "reference_truncated_anneal", "kwargs": {"test": test}, "method": method,
+            "timestep": 0.001, "t_end": 10.0 if test.endswith("_tl") else 1.0}
+    got, _ = run_oracle(case)
+    raw = got.T.reshape(-1)  # column-major, the reference's storage
+    assert np.abs(raw - expected).max() <= tol
