@@ -50,10 +50,11 @@ def parse_args():
     ap.add_argument("--impl", default="phi_b200", choices=["phi_b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="frenkel7", choices=["frenkel7", "ring24", "batched", "steady"],
+    ap.add_argument("--workload", default="frenkel7",
+                    choices=["frenkel7", "ring24", "batched", "steady", "spin_boson"],
                     help="frenkel7: the RKF45 headline (7-site exciton); ring24: 24-site ring RKF45; "
                          "batched: 512 uneven RK4 instances; steady: chain4 steady states, plain vs "
-                         "learned initial guess")
+                         "learned initial guess; spin_boson: the 11-node RK4 configuration")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--draws", type=int, default=32, help="steady workload: held-out draws")
     return ap.parse_args()
@@ -268,6 +269,113 @@ def run_reference_arm(args):
     return res
 
 
+def run_spin_boson(args):
+    """The spin-boson configuration (one Drude bath on sigma_z, DiagonalBath,
+    K = 0, L = 10: 11 nodes of 2x2; RK4 dt = 1 fs, 2000 steps = 2 ps, rho_0
+    every 10 fs).  The hierarchy is 44 complex numbers, so the run is bound
+    by latency, not by HBM or the SMs: the device runs it whole in one CTA
+    (heom_small.cu), one launch per 4096 steps.  A step is one RK4 step (4
+    Liouvillian applies over the hierarchy); value = node-applies/s of the
+    device-timed steps; e2e = the whole job through the C ABI from host
+    arrays (create, 2000 steps with the trajectory rows, read-back, destroy).
+    The reference arm runs the reference build with one thread, its fastest
+    setting for this size (the thread barriers of more threads cost more
+    than the 44 elements of work per stage)."""
+    import numpy as np
+    from phi_b200 import configs
+    p = configs.spin_boson()
+    dt, K = 0.001, args.steps if args.steps > 0 else 2000
+    M = configs.hierarchy_nodes(1, 10)
+    base = {"metric": "hierarchy-node applies/sec (RK4, spin-boson)", "unit": UNIT, "n_gpus": 1,
+            "steps": K, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic (spin-boson, fixed parameters)",
+            "config": {"workload": "spin_boson_L10 (11 nodes of 2x2, DiagonalBath, RK4 dt 1 fs)", "nodes": M,
+                       "parallelism": "single instance"}}
+    if args.impl == "reference":
+        from oracle import oracle as O
+        res = dict(base, impl="reference")
+        if not O.ref_available():
+            res["unavailable"] = "reference build oracle/_ref/ref_driver not present"
+            print(json.dumps(res), flush=True)
+            return
+
+        def wall(t_end):
+            best = float("inf")
+            for _ in range(3):
+                t0 = time.perf_counter()
+                O.run_reference(p, "rk4", 1, timeout=300, timestep=dt, t_end=t_end)
+                best = min(best, time.perf_counter() - t0)
+            return best
+        # Per step from the difference of two run lengths (process start and
+        # setup cancel).
+        long_steps, short_steps = 20 * K, 2 * K
+        per_step = (wall(long_steps * dt) - wall(short_steps * dt)) / (long_steps - short_steps)
+        value = 4 * M / per_step
+        res.update({"value": value, "ms_per_step": per_step * 1e3,
+                    "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                                     "cpu": cpu_model(),
+                                     "sample": f"reference build, RK4 runs of {long_steps} and {short_steps} steps "
+                                               f"(wall time difference, best of 3), 1 thread"},
+                    "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        print(json.dumps(res), flush=True)
+        return
+
+    import torch
+    from phi_b200 import capi
+    from phi_b200.heom import Hierarchy
+    h = Hierarchy(p)
+    stream = torch.cuda.ExternalStream(h.stream_handle())
+    h.rk4(dt, max(args.warmup, 3) * dt)
+    torch.cuda.synchronize()
+    sampler = ClockSampler(0)
+    sampler.start()
+    sampler.wait_first_sample()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h.rk4(dt, h.time + K * dt * (1 - 1e-9))
+    e1.record(stream)
+    e1.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    value = 4 * M * K / (ms / 1e3)
+    h.close()
+    # e2e: the user job of the configuration, warm process, second run reported.
+    rows = 200
+    for _ in range(2):
+        t0 = time.perf_counter()
+        h2 = Hierarchy(p)
+        h2.rk4(dt, K * dt, output_min_step=0.01, capacity=rows)
+        rho0 = h2.rho0()
+        h2.close()
+        e2e_s = time.perf_counter() - t0
+    from oracle import oracle as O
+    o = O.Oracle(p)
+    s_o, *_ = o.rk4(o.initial_state(), dt, K * dt)
+    err = float(np.abs(rho0 - o.rho0(s_o)).max())
+    t0 = time.perf_counter()
+    reps = 0
+    while time.perf_counter() - t0 < 5.0:
+        o.rk4(o.initial_state(), dt, K * dt)
+        reps += 1
+    cpu_s = (time.perf_counter() - t0) / reps
+    out = dict(base)
+    out.update({"value": value, "ms_per_step": ms / K,
+                "roofline": None,
+                "roofline_note": "latency-bound: 44 complex elements live in one CTA's shared memory for the "
+                                 "whole run (no HBM traffic per step); the bound is the per-stage barrier and "
+                                 "shared-memory latency",
+                "rho0_err_vs_oracle": err,
+                "e2e": {"value": 4 * M * K / e2e_s, "unit": UNIT, "seconds": e2e_s,
+                        "h2d_bytes_per_step": (2 * 4 + 2 * 4 + 2 + 2) * 8 / K,
+                        "d2h_bytes_per_step": (rows * 4 * 16 + 4 * 16) / K},
+                "cpu_baseline": {"value": 4 * M * K / cpu_s, "unit": UNIT, "cores": 1, "kind": "port",
+                                 "cpu": cpu_model(),
+                                 "sample": f"the oracle's C restatement, the whole {K}-step run x {reps}"},
+                "gpu_launches": (K + 4095) // 4096,
+                "clocks": clocks})
+    print(json.dumps(out), flush=True)
+
+
 def run_steps(h, steps, fresh):
     """Exactly `steps` attempted RKF45 steps of the 1 ps propagation; when a
     propagation reaches t_end it restarts from rho(0) on the device
@@ -462,6 +570,10 @@ def main():
                    "not timed for this workload: the reference integrates one problem per process "
                    "(its CPU path is timed on the frenkel7 and ring24 workloads)")
             print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return
+    if args.workload == "spin_boson":
+        if int(os.environ.get("RANK", "0")) == 0:
+            run_spin_boson(args)
         return
     if args.workload == "batched":
         run_batched(args)

@@ -56,4 +56,16 @@ cudaError_t launch_rkf45_control(Rkf45Ctl *ctl, cudaStream_t stream);
 cudaError_t launch_to_c64(const double2 *in, float2 *out, long long M, int E, int padded, cudaStream_t s);
 cudaError_t launch_to_c128(const float2 *in, double2 *out, long long M, int E, int padded, cudaStream_t s);
 
+// Small hierarchies (heom_small.cu): a whole FP64 RK4 run in one CTA with
+// the state in shared memory.  Eligible: IndependentBath or DiagonalBath
+// couplings the tiled kernel does not take, no filtering or time-local
+// truncation, at most kSmallMaxElements complex elements.  The caller excludes annealing and
+// mixed-precision contexts.  `steps` RK4 steps of dt on y in place, rho_0
+// rows and the step / row counters kept in rk4 as the stage kernels keep them.
+constexpr long long kSmallMaxElements = 2048;
+constexpr size_t kSmallMaxSmem = 200 * 1024;
+bool small_rk4_eligible(const HeomConsts &c);
+cudaError_t launch_small_rk4(const HeomConsts &c, double2 *y, double dt, long long steps, Rk4Ctl *rk4,
+                             double2 *traj, cudaStream_t stream);
+
 }  // namespace phi

@@ -297,19 +297,49 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
     // Hilbert-space truncation: restate the problem in the lowest num_states
     // eigenvectors of the Hamiltonian, then build an ordinary context.
     if (d.hilbert_space_size > 1024) return fail(nullptr, PHI_E_INVALID, "hilbert_space_size must be <= 1024");
-    if (!d.hamiltonian || !d.initial_density_matrix)
+    const bool anneal_t = d.annealing_h_x != nullptr;
+    if ((!d.hamiltonian && !anneal_t) || !d.initial_density_matrix)
       return fail(nullptr, PHI_E_INVALID, "hamiltonian and initial_density_matrix are required");
     const int F = d.hilbert_space_size;
     for (int k = 0; k < 2 * F * F; ++k)
-      if (!std::isfinite(d.hamiltonian[k]) || !std::isfinite(d.initial_density_matrix[k]))
+      if ((!anneal_t && !std::isfinite(d.hamiltonian[k])) || !std::isfinite(d.initial_density_matrix[k]))
         return fail(nullptr, PHI_E_INVALID, "non-finite value in the Hamiltonian or the initial density matrix");
     phi::TruncatedProblem t;
     std::string err;
     if (phi::truncate_problem(d, &t, &err) != 0) return fail(nullptr, PHI_E_INVALID, err);
     const int rc = phi_gpu_create(&t.desc, out);
     if (rc != PHI_OK) return rc;
-    (*out)->hilbert_full = F;
-    (*out)->trunc_basis = std::move(t.basis);
+    phi_ctx *ctx = *out;
+    ctx->hilbert_full = F;
+    ctx->trunc_basis = std::move(t.basis);
+    if (anneal_t) {
+      // The device re-diagonalises H(t) at every update: full H_X, H_Z, the
+      // current basis and the rotation of the last update live on the device.
+      static_assert(phi::kTruncatedAnnealingMaxFull == phi::kAnnealMaxFull, "eigensolver size");
+      const int k = ctx->desc.num_states;
+      const size_t fb = (size_t)F * F * sizeof(double);
+      std::vector<double> hx(t.hx_full), hz(t.hz_full);
+      cudaError_t e = cudaSuccess;
+      if (ctx->ta_hx.alloc(fb) != cudaSuccess || ctx->ta_hz.alloc(fb) != cudaSuccess ||
+          ctx->ta_V.alloc((size_t)F * k * sizeof(double)) != cudaSuccess ||
+          ctx->ta_R.alloc((size_t)k * k * sizeof(double)) != cudaSuccess ||
+          ctx->ta_rotate.alloc(sizeof(int)) != cudaSuccess)
+        e = cudaErrorMemoryAllocation;
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->ta_hx.ptr, hx.data(), fb, cudaMemcpyHostToDevice, ctx->stream);
+      if (e == cudaSuccess) e = cudaMemcpyAsync(ctx->ta_hz.ptr, hz.data(), fb, cudaMemcpyHostToDevice, ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // hx, hz are locals
+      if (e == cudaSuccess) {
+        ctx->ta_F = F;
+        ctx->ta_bath0 = ctx->coupling;  // the bath operators truncated into the initial basis
+        e = ctx->reset_annealing();
+      }
+      if (e != cudaSuccess) {
+        phi_gpu_destroy(ctx);
+        *out = nullptr;
+        return fail(nullptr, e == cudaErrorMemoryAllocation ? PHI_E_OOM : PHI_E_CUDA,
+                    std::string("truncated annealing setup: ") + cudaGetErrorString(e));
+      }
+    }
     return PHI_OK;
   }
   const bool annealing = d.annealing_h_x != nullptr;
@@ -566,6 +596,16 @@ cudaError_t phi_ctx::reset_annealing() {
   const phi::AnnealState st{DBL_MAX, DBL_MAX, 0, 0};  // numeric_limits<Float>::max() (:518-523)
   cudaError_t e = cudaMemcpyAsync(an_state.ptr, &st, sizeof(st), cudaMemcpyHostToDevice, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(cbuf.H.ptr, 0, cbuf.H.bytes, stream);
+  if (ta_F > 0) {
+    // Truncated: the initial basis and the bath operators truncated into it.
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(ta_V.ptr, trunc_basis.data(), trunc_basis.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess && !ta_bath0.empty())
+      e = cudaMemcpyAsync(cbuf.bath_V.ptr, ta_bath0.data(), ta_bath0.size() * sizeof(double),
+                          cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(ta_rotate.ptr, 0, sizeof(int), stream);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream);  // st is a local
   return e;
 }
@@ -589,7 +629,40 @@ cudaError_t phi_ctx::enqueue_anneal(int op, int which, double dt, cudaStream_t s
   L.E = desc.num_states * desc.num_states;
   L.integration_time = desc.integration_time;
   L.min_field_change = desc.minimum_field_change;
+  if (ta_F > 0) {
+    L.tr.F = ta_F;
+    L.tr.k = desc.num_states;
+    L.tr.hx = ta_hx.as<double>();
+    L.tr.hz = ta_hz.as<double>();
+    L.tr.V = ta_V.as<double>();
+    L.tr.R = ta_R.as<double>();
+    L.tr.rotate = static_cast<int *>(ta_rotate.ptr);
+    // PHI rotates the bath operators only when it reads them: more than one
+    // tier or time-local truncation (hierarchy_integrator.cc:1661-1668).
+    const bool bath = desc.bath_kind == PHI_BATH_FULL && (desc.truncation_level > 1 || desc.time_local);
+    L.tr.bath = bath ? cbuf.bath_V.as<double>() : nullptr;
+    L.tr.nb = bath ? desc.num_baths : 0;
+  }
   return phi::launch_anneal(L, s);
+}
+
+cudaError_t phi_ctx::enqueue_anneal_rotate(std::initializer_list<void *> bufs, bool rkf45_y, cudaStream_t s) {
+  if (ta_F == 0) return cudaSuccess;
+  phi::AnnealRotate r;
+  r.rotate = static_cast<const int *>(ta_rotate.ptr);
+  r.R = ta_R.as<double>();
+  r.k = desc.num_states;
+  r.M = hier.M;
+  for (void *b : bufs) {
+    if (r.nbuf == phi::kAnnealMaxRotate) return cudaErrorInvalidValue;
+    r.buf[r.nbuf++] = static_cast<double2 *>(b);
+  }
+  if (rkf45_y) {
+    r.ybuf[0] = y.as<double2>();
+    r.ybuf[1] = y_alt.as<double2>();
+    r.ctl = ctl.as<phi::Rkf45Ctl>();
+  }
+  return phi::launch_anneal_rotate(r, num_sms, s);
 }
 
 extern "C" int phi_gpu_get_hamiltonian(const phi_ctx *cctx, double *h) {
@@ -665,7 +738,13 @@ extern "C" int phi_gpu_get_rho0_full(const phi_ctx *cctx, double *rho0) {
   std::vector<double> rk(2 * (size_t)k * k);
   const int rc = phi_gpu_get_rho0(ctx, rk.data());
   if (rc != PHI_OK) return rc;
-  phi::untruncate(ctx->hilbert_full, k, ctx->trunc_basis.data(), rk.data(), rho0);
+  std::vector<double> basis(ctx->trunc_basis);
+  if (ctx->ta_F > 0) {  // an annealing run's basis follows H(t)
+    PHI_CUDA(ctx, cudaMemcpyAsync(basis.data(), ctx->ta_V.ptr, basis.size() * sizeof(double),
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  phi::untruncate(ctx->hilbert_full, k, basis.data(), rk.data(), rho0);
   return PHI_OK;
 }
 

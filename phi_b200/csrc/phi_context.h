@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <complex>
+#include <initializer_list>
 #include <string>
 #include <vector>
 
@@ -66,7 +67,8 @@ struct phi_ctx {
   int rk4_graph_steps = 0;
   double rk4_graph_dt = 0.0;
   void *rk4_graph_traj = nullptr;
-  cudaGraphExec_t rkf45_graph = nullptr;
+  cudaGraphExec_t rkf45_graph = nullptr;   // kGraphSteps steps
+  cudaGraphExec_t rkf45_graph1 = nullptr;  // one step
   int rkf45_graph_steps = 0;
 
   // Steady-state solve: x, rhat, b, r_0..r_ell, u_0..u_ell (complex128 state
@@ -96,6 +98,13 @@ struct phi_ctx {
   // (F x num_states, real); hilbert_full == num_states without truncation.
   int hilbert_full = 0;
   std::vector<double> trunc_basis;
+  // Truncated annealing (ta_F = F > 0): full H_X, H_Z (F x F real), the
+  // current basis (F x k), the rotation of the last update (k x k) and its
+  // flag, on the device; the bath operators truncated into the initial basis
+  // (host, for resets).  The initial basis is trunc_basis.
+  int ta_F = 0;
+  phi::DeviceBuffer ta_hx, ta_hz, ta_V, ta_R, ta_rotate;
+  std::vector<double> ta_bath0;
 
   double time = 0.0;
   std::string error;
@@ -127,6 +136,10 @@ struct phi_ctx {
   cudaError_t reset_annealing();
   // Enqueues one annealing update (no-op without annealing).
   cudaError_t enqueue_anneal(int op, int which, double dt, cudaStream_t s);
+  // Truncated annealing: rotates the listed live ADO arrays (complex128, M
+  // nodes each) and, with rkf45_y, the current RKF45 state into the basis
+  // of the last update (no-op without truncation or when it kept the basis).
+  cudaError_t enqueue_anneal_rotate(std::initializer_list<void *> bufs, bool rkf45_y, cudaStream_t s);
 };
 
 namespace phi {

@@ -39,6 +39,9 @@ int cuda_err(phi_ctx *ctx, cudaError_t e, const char *where) {
   } while (0)
 
 constexpr int kGraphSteps = 16;
+// Steps per launch of the one-CTA small-hierarchy RK4 kernel (bounds the
+// duration of one launch).
+constexpr long long kSmallChunk = 4096;
 
 }  // namespace
 
@@ -78,6 +81,8 @@ int phi_ctx::ensure_work(int level) {
 void phi_ctx::release_graphs() {
   if (rk4_graph) cudaGraphExecDestroy(rk4_graph);
   if (rkf45_graph) cudaGraphExecDestroy(rkf45_graph);
+  if (rkf45_graph1) cudaGraphExecDestroy(rkf45_graph1);
+  rkf45_graph1 = nullptr;
   if (bicg_graph) cudaGraphExecDestroy(bicg_graph);
   rk4_graph = nullptr;
   rkf45_graph = nullptr;
@@ -114,9 +119,18 @@ cudaError_t enqueue_rk4_step(phi_ctx *ctx, double dt, double2 *traj, int par, cu
       cudaError_t e = ctx->enqueue_time_local(phi::kTlAdvance, 0, dt / 2, s);
       if (e != cudaSuccess) return e;
     }
-    // Annealing Hamiltonian at t, t + dt/2 and t + dt (:2688, :2728, :2792).
+    // Annealing Hamiltonian at t, t + dt/2 and t + dt (:2688, :2728, :2792);
+    // under Hilbert-space truncation the live ADOs follow the basis (y at t;
+    // then y, the accumulator holding y and the k_s so far, and the stage
+    // input: :2693, :2733-2735, :2797-2801).
     if (st != 2) {
       cudaError_t e = ctx->enqueue_anneal(phi::kAnnealRk4, st == 0 ? 0 : (st == 1 ? 1 : 2), dt, s);
+      if (e == cudaSuccess) {
+        if (st == 0)
+          e = ctx->enqueue_anneal_rotate({ctx->y.ptr}, false, s);
+        else
+          e = ctx->enqueue_anneal_rotate({ctx->y.ptr, ctx->acc.ptr, ctx->xa.ptr}, false, s);
+      }
       if (e != cudaSuccess) return e;
     }
     L.stage = st;
@@ -158,9 +172,24 @@ cudaError_t enqueue_rkf45_step(phi_ctx *ctx, cudaStream_t s) {
       cudaError_t e = ctx->enqueue_time_local(phi::kTlRkf45Stage, st, 0.0, s);
       if (e != cudaSuccess) return e;
     }
-    // Annealing Hamiltonian at t + a_s (:1988, :2033, :2084, :2138, :2194, :2252).
+    // Annealing Hamiltonian at t + a_s (:1988, :2033, :2084, :2138, :2194, :2252);
+    // under Hilbert-space truncation the live ADOs follow the basis: y, the
+    // stage input and k_0..k_{s-1} (k_1 is not read after stage 4, :2259-2263).
     {
       cudaError_t e = ctx->enqueue_anneal(phi::kAnnealRkf45, st, 0.0, s);
+      if (e == cudaSuccess && ctx->ta_F > 0) {
+        void *x = const_cast<double2 *>(in[st]);
+        void *k0 = ctx->kbuf[0].ptr, *k1 = ctx->kbuf[1].ptr, *k2 = ctx->kbuf[2].ptr, *k3 = ctx->kbuf[3].ptr,
+             *k4 = ctx->kbuf[4].ptr;
+        switch (st) {
+          case 0: e = ctx->enqueue_anneal_rotate({}, true, s); break;
+          case 1: e = ctx->enqueue_anneal_rotate({x, k0}, true, s); break;
+          case 2: e = ctx->enqueue_anneal_rotate({x, k0, k1}, true, s); break;
+          case 3: e = ctx->enqueue_anneal_rotate({x, k0, k1, k2}, true, s); break;
+          case 4: e = ctx->enqueue_anneal_rotate({x, k0, k1, k2, k3}, true, s); break;
+          default: e = ctx->enqueue_anneal_rotate({x, k0, k2, k3, k4}, true, s); break;
+        }
+      }
       if (e != cudaSuccess) return e;
     }
     L.stage = st;
@@ -244,6 +273,23 @@ extern "C" int phi_gpu_rk4(phi_ctx *ctx, double dt, double t_end, double output_
   hc.nout = 0;
   PHI_CK(cudaMemcpyAsync(ctx->ctl.ptr, &hc, sizeof(hc), cudaMemcpyHostToDevice, ctx->stream));
 
+  // A small hierarchy runs whole in one CTA (launches of at most
+  // kSmallChunk steps each).
+  if (!ctx->annealing && !ctx->mixed() && phi::small_rk4_eligible(ctx->c)) {
+    for (long long done = 0; done < steps; done += kSmallChunk)
+      PHI_CK(phi::launch_small_rk4(ctx->c, ctx->y.as<double2>(), dt, std::min<long long>(kSmallChunk, steps - done),
+                                   ctx->ctl.as<phi::Rk4Ctl>(), dtraj, ctx->stream));
+    if (rows > 0)
+      PHI_CK(cudaMemcpyAsync(traj, dtraj, (size_t)rows * ctx->desc.num_states * ctx->desc.num_states * sizeof(double2),
+                             cudaMemcpyDeviceToHost, ctx->stream));
+    PHI_CK(cudaStreamSynchronize(ctx->stream));
+    if (times)
+      for (long long r = 0; r < std::min<long long>((long long)out_times.size(), capacity); ++r) times[r] = out_times[r];
+    ctx->time = t;
+    if (num_steps) *num_steps = steps;
+    if (num_out) *num_out = (int64_t)out_times.size();
+    return ctx->check_device_flag();
+  }
   // Replay a graph of kGraphSteps steps; the tail runs as direct launches.
   if (steps >= kGraphSteps &&
       (!ctx->rk4_graph || ctx->rk4_graph_dt != dt || ctx->rk4_graph_traj != (void *)dtraj)) {
@@ -344,6 +390,9 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
       }
       return cudaSuccess;
     }, &ctx->rkf45_graph));
+    // One step, for the remainder of a call (fewer launch calls and
+    // inter-kernel gaps than seven direct launches).
+    PHI_CK(capture(ctx->stream, [&]() { return enqueue_rkf45_step(ctx, ctx->stream); }, &ctx->rkf45_graph1));
   }
   if (!ctx->host_ctl) PHI_CK(phi::cached_host_alloc(&ctx->host_ctl, sizeof(phi::Rkf45Ctl)));
   phi::Rkf45Ctl *hpin = static_cast<phi::Rkf45Ctl *>(ctx->host_ctl);
@@ -361,7 +410,7 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
       return cudaGraphLaunch(ctx->rkf45_graph, ctx->stream);
     }
     for (; launched < hc.max_steps; ++launched) {
-      cudaError_t e = enqueue_rkf45_step(ctx, ctx->stream);
+      cudaError_t e = cudaGraphLaunch(ctx->rkf45_graph1, ctx->stream);
       if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -387,10 +436,20 @@ int run_rkf45(phi_ctx *ctx, double dt0, double t_end, double tol, double min_dt,
   if (result == PHI_OK) {
     hc = *hpin;
     if (hc.ycur == 1) {
-      std::swap(ctx->y, ctx->y_alt);
-      std::swap(ctx->y32, ctx->y32_alt);
-      std::swap(ctx->active[0], ctx->active[1]);
-      ctx->release_graphs();  // captured graphs bake in the y / y_alt pointers
+      // The current state is in the alternate buffers: copy it back on the
+      // device rather than swap the buffers, so the captured step graphs
+      // (which bake in both pointers) stay valid for the next call.
+      cudaError_t e = cudaMemcpyAsync(ctx->y.ptr, ctx->y_alt.ptr, ctx->state_bytes(), cudaMemcpyDeviceToDevice,
+                                      ctx->stream);
+      // (y32 is rebuilt from y at the start of every call.)
+      if (e == cudaSuccess && ctx->c.filtered)
+        e = cudaMemcpyAsync(ctx->active[0].ptr, ctx->active[1].ptr, (size_t)ctx->hier.M, cudaMemcpyDeviceToDevice,
+                            ctx->stream);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+      if (e != cudaSuccess) {
+        result = cuda_err(ctx, e, "rkf45 state copy");
+      }
+      hc.ycur = 0;
     }
     ctx->time = hc.time;
     ctx->rkf45_last = hc;

@@ -173,10 +173,18 @@ int put_tl_store(phi_ctx *ctx, const std::vector<double> &qk) {
   return PHI_OK;
 }
 
+// A truncated annealing run's ADOs are expressed in the basis of its last
+// Hamiltonian update, which a state file does not carry.
+int refuse_truncated_annealing(phi_ctx *ctx) {
+  ctx->error = "restart and state files of a Hilbert-space truncated annealing run are not built";
+  return fail(PHI_E_INVALID, ctx->error);
+}
+
 }  // namespace
 
 extern "C" int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->ta_F > 0) return refuse_truncated_annealing(ctx);
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -192,6 +200,7 @@ extern "C" int phi_gpu_write_restart(phi_ctx *ctx, const char *path, double time
 
 extern "C" int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->ta_F > 0) return refuse_truncated_annealing(ctx);
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -210,6 +219,7 @@ extern "C" int phi_gpu_read_restart(phi_ctx *ctx, const char *path, double *time
 
 extern "C" int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->ta_F > 0) return refuse_truncated_annealing(ctx);
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);
@@ -234,6 +244,7 @@ extern "C" int phi_gpu_save_state(phi_ctx *ctx, const char *path, double timeste
 
 extern "C" int phi_gpu_load_state(phi_ctx *ctx, const char *path, double *timestep) {
   if (!ctx || !path) return PHI_E_INVALID;
+  if (ctx->ta_F > 0) return refuse_truncated_annealing(ctx);
   int64_t M = 0;
   int32_t N = 0;
   phi_gpu_dims(ctx, &M, nullptr, &N);

@@ -1,4 +1,4 @@
-// phi_truncation.cpp -- Hilbert-space truncation of a static problem (host).
+// phi_truncation.cpp -- Hilbert-space truncation of a problem (host).
 //
 // PHI's HilbertSpaceTruncator (hilbert_space_truncator.cc:34-134) keeps the
 // lowest k eigenvectors V (F x k) of the full F x F Hamiltonian (LAPACK
@@ -123,9 +123,22 @@ void project(int F, int k, const double *A, const double *V, std::vector<double>
 int truncate_problem(const phi_problem_desc &d, TruncatedProblem *t, std::string *err) {
   const int F = d.hilbert_space_size, k = d.num_states;
   t->full = F;
-  if (d.annealing_h_x) {
-    *err = "Hilbert-space truncation of an annealing Hamiltonian is not built (static Hamiltonians only)";
-    return 1;
+  const bool annealing = d.annealing_h_x != nullptr;
+  if (annealing) {
+    if (F > kTruncatedAnnealingMaxFull) {
+      *err = "Hilbert-space truncation of an annealing Hamiltonian is built for hilbert_space_size <= " +
+             std::to_string(kTruncatedAnnealingMaxFull);
+      return 1;
+    }
+    if (d.precision != PHI_PREC_FP64) {
+      *err = "Hilbert-space truncation of an annealing Hamiltonian runs in FP64 (PHI_PREC_FP64)";
+      return 1;
+    }
+    if (!d.annealing_h_z || !d.transverse_field || !d.longitudinal_field || d.transverse_field_size < 1 ||
+        d.longitudinal_field_size < 1) {
+      *err = "an annealing Hamiltonian needs H_X, H_Z and both field arrays";
+      return 1;
+    }
   }
   if (d.truncation_level > 1 || d.time_local) {
     if (d.bath_kind != PHI_BATH_FULL || !d.coupling) {
@@ -135,20 +148,37 @@ int truncate_problem(const phi_problem_desc &d, TruncatedProblem *t, std::string
       return 1;
     }
   }
-  std::vector<double> H((size_t)F * F);
-  for (int e = 0; e < F * F; ++e) {
-    if (d.hamiltonian[2 * e + 1] != 0.0) {
-      *err = "Hilbert-space truncation is built for real symmetric Hamiltonians";
-      return 1;
-    }
-    H[e] = d.hamiltonian[2 * e];
-  }
-  for (int j = 0; j < F; ++j)
-    for (int i = 0; i < j; ++i)
-      if (H[i + (size_t)j * F] != H[j + (size_t)i * F]) {
-        *err = "the Hamiltonian is not symmetric";
-        return 1;
+  // The real symmetric F x F matrix of an interleaved complex one.
+  auto real_symmetric = [&](const double *m, const char *what, std::vector<double> *out) {
+    out->assign((size_t)F * F, 0.0);
+    for (int e = 0; e < F * F; ++e) {
+      if (!std::isfinite(m[2 * e]) || m[2 * e + 1] != 0.0) {
+        *err = std::string("Hilbert-space truncation is built for real symmetric Hamiltonians (") + what + ")";
+        return false;
       }
+      (*out)[e] = m[2 * e];
+    }
+    for (int j = 0; j < F; ++j)
+      for (int i = 0; i < j; ++i)
+        if ((*out)[i + (size_t)j * F] != (*out)[j + (size_t)i * F]) {
+          *err = std::string("the Hamiltonian is not symmetric (") + what + ")";
+          return false;
+        }
+    return true;
+  };
+  std::vector<double> H;
+  if (annealing) {
+    // The truncator is first updated with H at alpha = 0, where PHI's
+    // splines return the first samples (hierarchy_integrator.cc:934-946).
+    if (!real_symmetric(d.annealing_h_x, "H_X", &t->hx_full) ||
+        !real_symmetric(d.annealing_h_z, "H_Z", &t->hz_full))
+      return 1;
+    const double fx = d.transverse_field[0], fz = d.longitudinal_field[0];
+    H.resize((size_t)F * F);
+    for (int e = 0; e < F * F; ++e) H[e] = fx * t->hx_full[e] + fz * t->hz_full[e];
+  } else if (!real_symmetric(d.hamiltonian, "H", &H)) {
+    return 1;
+  }
   std::vector<double> w(F), V((size_t)F * F);
   if (jacobi_eigh(F, H.data(), w.data(), V.data()) != 0) {
     *err = "Jacobi eigenvalue iteration did not converge";
@@ -162,7 +192,15 @@ int truncate_problem(const phi_problem_desc &d, TruncatedProblem *t, std::string
   }
   t->basis.assign(V.begin(), V.begin() + (size_t)F * k);
   t->eigenvalues.assign(w.begin(), w.begin() + k);
-  project(F, k, d.hamiltonian, t->basis.data(), &t->hamiltonian);
+  if (annealing) {
+    std::vector<double> c((size_t)2 * F * F, 0.0);
+    for (int e = 0; e < F * F; ++e) c[2 * (size_t)e] = t->hx_full[e];
+    project(F, k, c.data(), t->basis.data(), &t->hx_k);
+    for (int e = 0; e < F * F; ++e) c[2 * (size_t)e] = t->hz_full[e];
+    project(F, k, c.data(), t->basis.data(), &t->hz_k);
+  } else {
+    project(F, k, d.hamiltonian, t->basis.data(), &t->hamiltonian);
+  }
   project(F, k, d.initial_density_matrix, t->basis.data(), &t->initial_density_matrix);
   t->coupling.clear();
   if (d.bath_kind == PHI_BATH_FULL && d.coupling) {
@@ -176,7 +214,11 @@ int truncate_problem(const phi_problem_desc &d, TruncatedProblem *t, std::string
   }
   t->desc = d;
   t->desc.hilbert_space_size = k;
-  t->desc.hamiltonian = t->hamiltonian.data();
+  t->desc.hamiltonian = annealing ? nullptr : t->hamiltonian.data();
+  if (annealing) {
+    t->desc.annealing_h_x = t->hx_k.data();
+    t->desc.annealing_h_z = t->hz_k.data();
+  }
   t->desc.initial_density_matrix = t->initial_density_matrix.data();
   t->desc.coupling = t->coupling.empty() ? nullptr : t->coupling.data();
   if (d.truncation_level == 1 && !d.time_local) {

@@ -93,3 +93,21 @@ def test_oracle_passes_reference_truncated_anneal_tests(test, method, expected, 
     got, _ = run_oracle(case)
     raw = got.T.reshape(-1)  # column-major, the reference's storage
     assert np.abs(raw - expected).max() <= tol
+
+
+def test_truncated_annealing_scope_checks_need_no_gpu():
+    from phi_b200 import capi
+    from phi_b200.heom import Hierarchy
+    p = cases.truncated_annealed(full=4, k=2, seed=1)
+    with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
+        Hierarchy(p, precision=capi.PHI_PREC_MIXED)  # FP64 only
+    p = cases.truncated_annealed(full=33, k=2, seed=1)
+    with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
+        Hierarchy(p)  # beyond the device eigensolver's 32
+    p = cases.truncated_annealed(full=4, k=2, seed=1)
+    hx = np.array(p.transverse_hamiltonian)
+    hx[0, 1] += 1j
+    hx[1, 0] -= 1j
+    p.transverse_hamiltonian = hx
+    with pytest.raises(capi.PhiError, match="PHI_E_INVALID"):
+        Hierarchy(p)  # complex H_X: not built
