@@ -4,10 +4,12 @@
 // tile_pairs / tile_epilogue of heom_tile_body.cuh.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstring>
 
 #include "heom_tile_body.cuh"
+#include "heom_umma.cuh"
 
 namespace phi {
 
@@ -36,6 +38,18 @@ struct TileBlock {
 // pair list, c_t, the dephasing rates and the prefactor tables are staged
 // once per CTA.  Three mbarriers: one per slot (phase parity (i >> 1) & 1 for
 // the CTA's i-th tile) and one for the epilogue operands (parity i & 1).
+// Tensor-core products (heom_umma.cuh) in the 24-site mixed kernel: with a
+// real H the tile's A = H X is one TF32 GEMM per tile, rows (node, column j
+// of X, re / im) x K = the row index i of X, against B = H (rows padded to
+// kTcRowsB), split into hi and lo parts; the CUDA cores then only combine
+// A_ij and A_ji per pair.  M = 128 rows (the tile's 2 x 24 x 2 = 96 rows and
+// 32 rows that alias the operand after them and whose results are unused).
+template <int N, bool MIXED>
+struct TileTc {
+  static constexpr bool on = MIXED && N == 24;
+  static constexpr int kM = 128, kRowsB = 32;
+};
+
 template <int N, int KT, bool MIXED, int BT>
 struct PipeLayout {
   using S = TileShape<N, MIXED, KT, BT>;
@@ -54,8 +68,15 @@ struct PipeLayout {
   static constexpr size_t kSlotMi = r16((size_t)S::NT * T + 32);
   static constexpr size_t kSlotDeph = r16(((size_t)S::NT + 2) * 8);  // per-node dephasing rates
   static constexpr size_t kSlot = r128(kSlotX + 2 * kSlotIds + kSlotMi + kSlotDeph);
-  static constexpr size_t kSlots = 128;                       // after the 3 mbarriers
-  static constexpr size_t kUs = kSlots + 2 * kSlot;           // derivative tile
+  static constexpr size_t kSlots = 128;                       // after the 4 mbarriers and the TMEM slot
+  // Tensor-core operands: A hi, A lo (the tile's rows), B hi, B lo (kRowsB
+  // rows); rows past a region's end read the next region.
+  static constexpr bool kTcOn = TileTc<N, MIXED>::on;
+  static constexpr size_t kTcRowsA = (size_t)S::NT * 2 * N;
+  static constexpr size_t kTcA = kTcOn ? kTcRowsA / 8 * (size_t)umma::kSbo<N> : 0;
+  static constexpr size_t kTcB = kTcOn ? (size_t)TileTc<N, MIXED>::kRowsB / 8 * (size_t)umma::kSbo<N> : 0;
+  static constexpr size_t kTc = kSlots + 2 * kSlot;
+  static constexpr size_t kUs = kTc + r128(2 * kTcA + 2 * kTcB);  // derivative tile
   static constexpr size_t kPre = kUs + r128((size_t)S::NT * S::EU * XB);
 };
 
@@ -119,11 +140,32 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
   unsigned char *pi = reinterpret_cast<unsigned char *>(nts + NT * T);
   unsigned char *pj = pi + P;
 
+  constexpr bool TC = Lay::kTcOn;
+  static_assert(!TC || Lay::kTcRowsA <= TileTc<N, MIXED>::kM, "tile rows fit one MMA");
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 4);
+  unsigned char *TcAhi = smem_raw + Lay::kTc, *TcAlo = TcAhi + Lay::kTcA;
+  unsigned char *TcBhi = TcAlo + Lay::kTcA, *TcBlo = TcBhi + Lay::kTcB;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     mbar_init(&bars[2], 1);
+    mbar_init(&bars[3], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  // The tensor-core path needs a real H (every in-scope 24-site workload).
+  const bool tc = TC && c.h_real;
+  if (tc) {
+    if (tid < 32) umma::tmem_alloc(tmem_slot, 32);
+    // B = H, row r = (H_r0 .. H_r,N-1), rows N .. kRowsB-1 zero, hi / lo.
+    for (int q = tid; q < TileTc<N, MIXED>::kRowsB * N; q += BT) {
+      const int r = q / N, k = q - r * N;
+      const float v = r < N ? (float)__ldg(c.H + r + k * N).x : 0.0f;
+      const float h = umma::tf32_hi(v);
+      *reinterpret_cast<float *>(TcBhi + umma::core_offset<N>(r, k)) = h;
+      *reinterpret_cast<float *>(TcBlo + umma::core_offset<N>(r, k)) = v - h;
+    }
+    umma::fence_async_smem();
+    umma::fence_before_sync();
   }
   int ycur = 0;
   if (p.mode == kModeRkf45) {
@@ -156,6 +198,11 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
     sqp[q] = (R)__ldg(c.sq_prev + q);
   }
   __syncthreads();  // barriers initialised, constants visible
+  uint32_t tmem = 0;
+  if (tc) {
+    umma::fence_after_sync();
+    tmem = *tmem_slot;
+  }
 
   const long long ntiles = (c.M + NT - 1) / NT;
   const TX *xin;
@@ -212,7 +259,7 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
   if (tid == 0 && tile < ntiles) issue_slot(tile, 0);
   double emax = 0.0;
   int i = 0;
-  bool failed = false, next_issued = false;
+  bool failed = false, next_issued = false, mma_inflight = false;
   for (; tile < ntiles; ++i, tile += gridDim.x) {
     const int s = i & 1;
     const long long n0 = tile * NT;
@@ -236,6 +283,38 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
     const uint8_t *mi_s = sb + Lay::kSlotX + 2 * Lay::kSlotIds + q0;
     const double *deph =
         reinterpret_cast<const double *>(sb + Lay::kSlotX + 2 * Lay::kSlotIds + Lay::kSlotMi) + (n0 & 1);
+    if (TC && tc) {
+      // Tensor-core operand A: row (node, j, re / im) = nd * 2N + 2j + c,
+      // K = i, element X_ij's component c, split into hi and lo.
+      for (int e = tid; e < nt_here * 2 * E; e += BT) {
+        const int row = e / N, ii = e - row * N;
+        const int nd = row / (2 * N), rem = row - nd * 2 * N, j = rem >> 1;
+        const TX x = Xs[nd * ES + ii + j * N];
+        const float v = (rem & 1) ? (float)x.y : (float)x.x;
+        const float h = umma::tf32_hi(v);
+        *reinterpret_cast<float *>(TcAhi + umma::core_offset<N>(row, ii)) = h;
+        *reinterpret_cast<float *>(TcAlo + umma::core_offset<N>(row, ii)) = v - h;
+      }
+      umma::fence_async_smem();
+      __syncthreads();
+      // D = A_hi B_hi^T + A_lo B_hi^T + A_hi B_lo^T in TMEM (lane = row,
+      // column = r); it runs while the threads prepare the neighbour records.
+      if (tid == 0) {
+        umma::fence_after_sync();
+        constexpr uint32_t idesc = umma::instr_desc_tf32(TileTc<N, MIXED>::kM, TileTc<N, MIXED>::kRowsB);
+        int n = 0;
+#pragma unroll
+        for (int pass = 0; pass < 3; ++pass) {
+          const unsigned char *a = pass == 1 ? TcAlo : TcAhi, *b = pass == 2 ? TcBlo : TcBhi;
+#pragma unroll
+          for (int ks = 0; ks < N / 8; ++ks, ++n)
+            umma::mma_tf32(tmem, umma::smem_desc<N>(a + ks * 2 * umma::kLbo), umma::smem_desc<N>(b + ks * 2 * umma::kLbo),
+                           idesc, n > 0);
+        }
+        umma::commit(&bars[3]);
+      }
+      mma_inflight = true;
+    }
     for (int q = tid; q < nt_here * T; q += BT) {
       const int nd = q / T, t = q - nd * T;
       const int nx = nx_s[q], pv = pv_s[q], nt = mi_s[q];
@@ -248,7 +327,37 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
       cp[q] = sqp[t * W + nt];
     }
     __syncthreads();
-    tile_pairs<N, KT, MIXED, BT>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
+    if (TC && tc) {
+      // Each row's A = H X values from TMEM into the derivative tile.
+      if (!__syncthreads_and(mbar_wait_bounded(&bars[3], (uint32_t)i & 1u))) {
+        failed = true;
+        break;
+      }
+      mma_inflight = false;
+      umma::fence_after_sync();
+      const int warp = tid >> 5;
+      if (warp < (int)(Lay::kTcRowsA + 31) / 32) {
+        const uint32_t base = tmem + ((uint32_t)(warp * 32) << 16);
+        uint32_t v16[16], v8[8];
+        umma::ld_x16(base, v16);
+        umma::ld_x8(base + 16, v8);
+        umma::wait_ld();
+        const int row = warp * 32 + (tid & 31);
+        if (row < nt_here * 2 * N) {
+          const int nd = row / (2 * N), rem = row - nd * 2 * N, j = rem >> 1, cc = rem & 1;
+          float *u = reinterpret_cast<float *>(Us + nd * S::EU + j * S::NP) + cc;
+#pragma unroll
+          for (int r = 0; r < 16; ++r) u[2 * r] = __uint_as_float(v16[r]);
+#pragma unroll
+          for (int r = 0; r < 8; ++r) u[2 * (16 + r)] = __uint_as_float(v8[r]);
+        }
+      }
+      umma::fence_before_sync();
+      __syncthreads();
+      tile_pairs<N, KT, MIXED, BT, true>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
+    } else {
+      tile_pairs<N, KT, MIXED, BT>(c, Xs, Us, Hs, mats, pi, pj, ids, cn, cp, ccr, deph, nts, xin, nt_here);
+    }
     if (!__syncthreads_and(p.npre == 0 || mbar_wait_bounded(&bars[2], (uint32_t)i & 1u))) {
       failed = true;
       break;
@@ -265,9 +374,20 @@ __global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
     mbar_wait_bounded(&bars[s], (uint32_t)(i >> 1) & 1u);
     if (next_issued) mbar_wait_bounded(&bars[s ^ 1], (uint32_t)((i + 1) >> 1) & 1u);
     if (p.npre > 0) mbar_wait_bounded(&bars[2], (uint32_t)i & 1u);
+    if (TC && tc) {
+      if (mma_inflight) mbar_wait_bounded(&bars[3], (uint32_t)i & 1u);
+      umma::fence_before_sync();
+      __syncthreads();
+      if (tid < 32) umma::tmem_dealloc(tmem, 32);
+    }
     return;
   }
   if (p.mode == kModeRkf45 && p.stage == 5) tile_error_max<MIXED, BT>(p, emax, wmax);
+  if (TC && tc) {
+    umma::fence_before_sync();
+    __syncthreads();
+    if (tid < 32) umma::tmem_dealloc(tmem, 32);
+  }
 }
 
 // Resident CTAs per SM of a kernel at a dynamic shared-memory size and the
@@ -294,6 +414,30 @@ int persistent_grid(const void *fn, int threads, size_t smem) {
   return grid;
 }
 
+// The same for a kernel that allocates tensor memory, whose occupancy the
+// runtime's calculator reports as one CTA per SM: resident CTAs from the
+// SM's shared memory (with the per-CTA reservation), its thread slots, and
+// the register budget the kernel was compiled for (at least min_blocks).
+// Measured on B200 with the 24-site kernel: two such CTAs per SM run
+// together (RKF45 step 2.31 ms with one per SM, 1.36 ms with two).
+int persistent_grid_tmem(int threads, size_t smem, int min_blocks) {
+  static thread_local int cached_dev = -1, sms = 0, smem_sm = 0, reserved = 0, threads_sm = 0;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (dev != cached_dev) {
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&threads_sm, cudaDevAttrMaxThreadsPerMultiProcessor, dev) != cudaSuccess)
+      return 0;
+    cached_dev = dev;
+  }
+  int blocks = (int)((size_t)smem_sm / (smem + (size_t)reserved));
+  blocks = std::min(blocks, threads_sm / threads);
+  blocks = std::min(blocks, std::max(min_blocks, 1));
+  return sms * std::max(blocks, 1);
+}
+
 template <int N, int KT, bool MIXED>
 cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
   constexpr int BT = TileBlock<N, MIXED>::threads;
@@ -306,7 +450,9 @@ cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
   cudaError_t e = raise_smem_limit(kern, smem_max, configured);
   if (e != cudaSuccess) return e;
   const size_t smem = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, p.npre, p.pre_bytes);
-  const int cap = persistent_grid((const void *)kern, BT, smem);
+  const int cap = TileTc<N, MIXED>::on
+                      ? persistent_grid_tmem(BT, smem, TileMinBlocks<KT, MIXED, BT>::value)
+                      : persistent_grid((const void *)kern, BT, smem);
   if (cap <= 0) return cudaErrorInvalidConfiguration;
   const long long grid = tiles < cap ? tiles : cap;
   kern<<<(unsigned)grid, BT, smem, stream>>>(p);

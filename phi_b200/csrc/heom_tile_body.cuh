@@ -242,8 +242,11 @@ struct TileArith {
 // the derivative tile Us, from shared memory (the tile's stage input Xs, H,
 // per-element Matsubara factors, pair lists, per-(node, term) neighbour
 // offsets and prefactor magnitudes, dephasing rates) and, for the neighbour
-// terms, from the stage input in HBM (xin).
-template <int N, int KT, bool MIXED, int BT>
+// terms, from the stage input in HBM (xin).  HX_US: the products A = H X of
+// the tile are already in Us (computed on the tensor cores); each item reads
+// its two entries A_ij, A_ji there before it overwrites them with the
+// derivative (no other item touches those two slots).
+template <int N, int KT, bool MIXED, int BT, bool HX_US = false>
 __device__ __forceinline__ void tile_pairs(const HeomConsts &c, const typename TileArith<MIXED>::TX *Xs,
                                            typename TileArith<MIXED>::TX *Us,
                                            const typename TileArith<MIXED>::TX *Hs,
@@ -269,7 +272,13 @@ __device__ __forceinline__ void tile_pairs(const HeomConsts &c, const typename T
     const int i = pi[u], j = pj[u];
     const TX *X = Xs + nd * ES;
     R ar = 0, ai = 0, br = 0, bi = 0;  // A_ij, A_ji
-    if (hreal) {
+    if (HX_US) {
+      const TX aij = Us[nd * EU + i + j * NP], aji = Us[nd * EU + j + i * NP];
+      ar = aij.x;
+      ai = aij.y;
+      br = aji.x;
+      bi = aji.y;
+    } else if (hreal) {
 #pragma unroll
       for (int k = 0; k < N; ++k) {
         // X_ki = conj(X_ik) (Hermitian ADO): lanes with consecutive i read
