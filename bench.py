@@ -612,6 +612,7 @@ def main():
     h = Hierarchy(p, precision=prec, device=local_rank)
     M = h.num_nodes
     T_terms = h.num_terms
+    tile_sched = h.tile_schedule()
     stream = torch.cuda.ExternalStream(h.stream_handle(), device=local_rank)
     run_steps(h, args.warmup, True)
     torch.cuda.synchronize()
@@ -749,6 +750,7 @@ def main():
                        "l2": f"working set 9 x {M * E * 16 / 1e6:.1f} MB state buffers = "
                              f"{9 * M * E * 16 / 1e6:.0f} MB > 126 MB L2"},
             "rkf45_steps_per_s": total_steps / (t_max / 1e3),
+            "tile_schedule": tile_sched,
             "rho0_err_vs_fp64": rho_err,
             "rho0_err_vs_reference": vs_ref,
             "meets_1e-6": rho_err <= 1e-6 and (vs_ref is None or vs_ref["mixed"] <= 1e-6),

@@ -275,6 +275,25 @@ enum {
 PHI_API int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
                                  const double *guess, phi_solve_stats *stats);
 
+/* Schedule of the tiled stage kernel (IndependentBath on PHI's identity site
+ * map, K + 1 <= 3, N in {2..8, 10, 12, 16, 24}).  phi_gpu_create times one
+ * Liouvillian apply for each block size (the shape's default and one
+ * alternative) and each cap on persistent CTAs per SM, for problems of at
+ * least 2^20 complex elements, and keeps the fastest (once per device,
+ * shape and size class in the process).  Results do not depend on the
+ * schedule, only the time.  threads = 0: the problem runs on the generic
+ * kernel.  ctas_per_sm = 0: as many as fit. */
+typedef struct {
+  int32_t threads;
+  int32_t ctas_per_sm;
+  double ms_per_apply;         /* the chosen schedule (0 if not tuned) */
+  double ms_per_apply_default; /* the default schedule (0 if not tuned) */
+} phi_tile_schedule;
+PHI_API int phi_gpu_get_tile_schedule(const phi_ctx *ctx, phi_tile_schedule *out);
+/* Sets the schedule: threads one of the two block sizes of the shape,
+ * ctas_per_sm >= 0.  PHI_E_INVALID otherwise or off the tiled kernel. */
+PHI_API int phi_gpu_set_tile_schedule(phi_ctx *ctx, int32_t threads, int32_t ctas_per_sm);
+
 /* rho_0 in the full Hilbert space, V rho_0 V^+ (UnTruncate,
  * hilbert_space_truncator.cc:82-95; hierarchy_integrator.cc:177-191): host
  * buffer of 2*F*F doubles, F = hilbert_space_size (the same as

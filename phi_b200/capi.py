@@ -86,6 +86,15 @@ class PhiRkf45Stats(ctypes.Structure):
     ]
 
 
+class PhiTileSchedule(ctypes.Structure):
+    _fields_ = [
+        ("threads", c_int32),
+        ("ctas_per_sm", c_int32),
+        ("ms_per_apply", c_double),
+        ("ms_per_apply_default", c_double),
+    ]
+
+
 class PhiSolveStats(ctypes.Structure):
     _fields_ = [
         ("iterations", c_int32),
@@ -120,6 +129,8 @@ SIGNATURES = [
     ("phi_gpu_dims", c_int, [c_void_p, POINTER(c_int64), POINTER(c_int32), POINTER(c_int32)]),
     ("phi_gpu_get_rho0_full", c_int, [c_void_p, c_void_p]),
     ("phi_gpu_hilbert_space_size", c_int, [c_void_p, POINTER(c_int32)]),
+    ("phi_gpu_get_tile_schedule", c_int, [c_void_p, POINTER(PhiTileSchedule)]),
+    ("phi_gpu_set_tile_schedule", c_int, [c_void_p, c_int32, c_int32]),
     ("phi_gpu_num_baths", c_int, [c_void_p, POINTER(c_int32)]),
     ("phi_gpu_get_node_table", c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     ("phi_gpu_set_state", c_int, [c_void_p, c_void_p]),

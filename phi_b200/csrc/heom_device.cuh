@@ -76,6 +76,11 @@ struct HeomConsts {
   // built-in limit, < 0 give up at once (a test of the timeout path; the
   // drain of the CTA's own copies keeps the built-in limit).
   long long first_wait_polls;
+  // Tile-kernel schedule (host side only, chosen by the autotuner):
+  // block-size variant (0 the default of the shape, 1 the alternative) and
+  // persistent CTAs per SM (0: as many as fit).
+  int tile_variant;
+  int tile_cps;
   // Adaptive hierarchy filtering (PHI's FilterTolerance, independent baths):
   // a node whose largest |element| drops below filter_tol stops feeding its
   // neighbours until it rises above it again.

@@ -25,6 +25,8 @@ namespace {
 template <int N, bool MIXED>
 struct TileBlock {
   static constexpr int threads = (MIXED && N == 24) ? 320 : kTileThreads;
+  // The autotuner's alternative block size (heom_tile.cu, tile_autotune).
+  static constexpr int alt = threads == kTileThreads ? 320 : kTileThreads;
 };
 
 // ---- persistent pipelined kernel ----
@@ -96,11 +98,8 @@ size_t pipe_smem(int T, int L, int npre, const int *pre_bytes) {
   return b;
 }
 
-template <int N, int KT, bool MIXED>
-__global__ void __launch_bounds__(TileBlock<N, MIXED>::threads,
-                                  TileMinBlocks<KT, MIXED, TileBlock<N, MIXED>::threads>::value)
-    heom_tile_pipe_kernel(TileParams p) {
-  constexpr int BT = TileBlock<N, MIXED>::threads;
+template <int N, int KT, bool MIXED, int BT>
+__global__ void __launch_bounds__(BT, TileMinBlocks<KT, MIXED, BT>::value) heom_tile_pipe_kernel(TileParams p) {
   using S = TileShape<N, MIXED, KT, BT>;
   using Lay = PipeLayout<N, KT, MIXED, BT>;
   using TX = typename TileArith<MIXED>::TX;
@@ -438,51 +437,67 @@ int persistent_grid_tmem(int threads, size_t smem, int min_blocks) {
   return sms * std::max(blocks, 1);
 }
 
-template <int N, int KT, bool MIXED>
-cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream) {
-  constexpr int BT = TileBlock<N, MIXED>::threads;
+// Launch of one block-size variant.  The grid is the resident-CTA count of
+// this launch's shared-memory size (capped at tile_cps CTAs per SM when the
+// schedule sets it) and never more than the tiles.  *per_sm (optional)
+// receives the resident CTAs per SM before the cap.
+template <int N, int KT, bool MIXED, int BT>
+cudaError_t launch_tile_bt(const TileParams &p, cudaStream_t stream, int *per_sm = nullptr) {
   using S = TileShape<N, MIXED, KT, BT>;
   const long long tiles = (p.c.M + S::NT - 1) / S::NT;
   const int max_bytes[kMaxPre] = {16, 16, 16, 16, 16};
   const size_t smem_max = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, kMaxPre, max_bytes);
-  auto kern = heom_tile_pipe_kernel<N, KT, MIXED>;
+  auto kern = heom_tile_pipe_kernel<N, KT, MIXED, BT>;
   static thread_local int configured[kSmemLimitDevices] = {};
   cudaError_t e = raise_smem_limit(kern, smem_max, configured);
   if (e != cudaSuccess) return e;
   const size_t smem = pipe_smem<N, KT, MIXED, BT>(p.c.T, p.c.L, p.npre, p.pre_bytes);
-  const int cap = TileTc<N, MIXED>::on
-                      ? persistent_grid_tmem(BT, smem, TileMinBlocks<KT, MIXED, BT>::value)
-                      : persistent_grid((const void *)kern, BT, smem);
+  int cap = TileTc<N, MIXED>::on ? persistent_grid_tmem(BT, smem, TileMinBlocks<KT, MIXED, BT>::value)
+                                 : persistent_grid((const void *)kern, BT, smem);
   if (cap <= 0) return cudaErrorInvalidConfiguration;
+  int sms = 0, dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return cudaErrorInvalidDevice;
+  if (per_sm) *per_sm = cap / sms;
+  if (p.c.tile_cps > 0 && p.c.tile_cps * sms < cap) cap = p.c.tile_cps * sms;
   const long long grid = tiles < cap ? tiles : cap;
   kern<<<(unsigned)grid, BT, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
+template <int N, int KT, bool MIXED>
+cudaError_t launch_tile_nk(const TileParams &p, cudaStream_t stream, int *per_sm = nullptr) {
+  // The steady-state apply writes one partial inner product per tile into
+  // an array sized by tile_count, i.e. by the default block's tiles.
+  if (p.c.tile_variant == 1 && !p.dot_w)
+    return launch_tile_bt<N, KT, MIXED, TileBlock<N, MIXED>::alt>(p, stream, per_sm);
+  return launch_tile_bt<N, KT, MIXED, TileBlock<N, MIXED>::threads>(p, stream, per_sm);
+}
+
 template <int N, bool MIXED>
-cudaError_t launch_tile_n(const TileParams &p, cudaStream_t stream) {
+cudaError_t launch_tile_n(const TileParams &p, cudaStream_t stream, int *per_sm) {
   switch (p.c.K1) {
-    case 1: return launch_tile_nk<N, 1, MIXED>(p, stream);
-    case 2: return launch_tile_nk<N, 2, MIXED>(p, stream);
-    case 3: return launch_tile_nk<N, 3, MIXED>(p, stream);
+    case 1: return launch_tile_nk<N, 1, MIXED>(p, stream, per_sm);
+    case 2: return launch_tile_nk<N, 2, MIXED>(p, stream, per_sm);
+    case 3: return launch_tile_nk<N, 3, MIXED>(p, stream, per_sm);
     default: return cudaErrorInvalidValue;
   }
 }
 
 template <bool MIXED>
-cudaError_t launch_tile_dispatch(const TileParams &p, cudaStream_t stream) {
+cudaError_t launch_tile_dispatch(const TileParams &p, cudaStream_t stream, int *per_sm = nullptr) {
   switch (p.c.N) {
-    case 2: return launch_tile_n<2, MIXED>(p, stream);
-    case 3: return launch_tile_n<3, MIXED>(p, stream);
-    case 4: return launch_tile_n<4, MIXED>(p, stream);
-    case 5: return launch_tile_n<5, MIXED>(p, stream);
-    case 6: return launch_tile_n<6, MIXED>(p, stream);
-    case 7: return launch_tile_n<7, MIXED>(p, stream);
-    case 8: return launch_tile_n<8, MIXED>(p, stream);
-    case 10: return launch_tile_n<10, MIXED>(p, stream);
-    case 12: return launch_tile_n<12, MIXED>(p, stream);
-    case 16: return launch_tile_n<16, MIXED>(p, stream);
-    case 24: return launch_tile_n<24, MIXED>(p, stream);
+    case 2: return launch_tile_n<2, MIXED>(p, stream, per_sm);
+    case 3: return launch_tile_n<3, MIXED>(p, stream, per_sm);
+    case 4: return launch_tile_n<4, MIXED>(p, stream, per_sm);
+    case 5: return launch_tile_n<5, MIXED>(p, stream, per_sm);
+    case 6: return launch_tile_n<6, MIXED>(p, stream, per_sm);
+    case 7: return launch_tile_n<7, MIXED>(p, stream, per_sm);
+    case 8: return launch_tile_n<8, MIXED>(p, stream, per_sm);
+    case 10: return launch_tile_n<10, MIXED>(p, stream, per_sm);
+    case 12: return launch_tile_n<12, MIXED>(p, stream, per_sm);
+    case 16: return launch_tile_n<16, MIXED>(p, stream, per_sm);
+    case 24: return launch_tile_n<24, MIXED>(p, stream, per_sm);
     default: return cudaErrorInvalidValue;
   }
 }
@@ -583,6 +598,70 @@ TileParams tile_params_for(const StageLaunch &L) {
 cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream) {
   const TileParams p = tile_params_for(L);
   return L.mixed ? launch_tile_dispatch<true>(p, stream) : launch_tile_dispatch<false>(p, stream);
+}
+
+namespace {
+template <bool MIXED>
+int block_threads_n(int N, int variant) {
+  switch (N) {
+#define PHI_TB(n) \
+  case n: return variant == 1 ? TileBlock<n, MIXED>::alt : TileBlock<n, MIXED>::threads;
+    PHI_TB(2) PHI_TB(3) PHI_TB(4) PHI_TB(5) PHI_TB(6) PHI_TB(7) PHI_TB(8) PHI_TB(10) PHI_TB(12) PHI_TB(16) PHI_TB(24)
+#undef PHI_TB
+    default: return 0;
+  }
+}
+}  // namespace
+
+int tile_block_threads(const HeomConsts &c, bool mixed, int variant) {
+  return mixed ? block_threads_n<true>(c.N, variant) : block_threads_n<false>(c.N, variant);
+}
+
+cudaError_t tile_autotune(const StageLaunch &L0, cudaStream_t stream, TileSchedule *out) {
+  StageLaunch L = L0;
+  L.mode = kModeApply;
+  L.dot_w = nullptr;
+  L.dot_part = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  TileSchedule best{};
+  best.ms = 1e30f;
+  float ms_default = 0.f;
+  constexpr int kReps = 3;
+  for (int variant = 0; variant < 2 && e == cudaSuccess; ++variant) {
+    L.c.tile_variant = variant;
+    L.c.tile_cps = 0;
+    int per_sm = 0;
+    TileParams p = tile_params_for(L);
+    // warm-up launch (module load, smem attribute) and the occupancy
+    e = L.mixed ? launch_tile_dispatch<true>(p, stream, &per_sm) : launch_tile_dispatch<false>(p, stream, &per_sm);
+    for (int cps = per_sm; cps >= 1 && e == cudaSuccess; --cps) {
+      p.c.tile_cps = cps == per_sm ? 0 : cps;
+      e = cudaEventRecord(e0, stream);
+      for (int r = 0; r < kReps && e == cudaSuccess; ++r)
+        e = L.mixed ? launch_tile_dispatch<true>(p, stream) : launch_tile_dispatch<false>(p, stream);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      ms /= kReps;
+      if (variant == 0 && cps == per_sm) ms_default = ms;
+      if (ms < best.ms) {
+        best.ms = ms;
+        best.variant = variant;
+        best.cps = p.c.tile_cps;
+      }
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (e != cudaSuccess) return e;
+  best.ms_default = ms_default;
+  best.threads = tile_block_threads(L.c, L.mixed, best.variant);
+  *out = best;
+  return cudaSuccess;
 }
 
 namespace {

@@ -13,6 +13,21 @@ cudaError_t launch_tile_stage(const StageLaunch &L, cudaStream_t stream);
 // Node stride of complex64 buffers (N*N rounded up to even).
 int mixed_node_stride(int N);
 
+// Schedule of the single-instance tile kernel: block-size variant (0 the
+// shape's default, 1 the alternative), persistent CTAs per SM (0: as many as
+// fit), with the measured apply times of the choice and of the default.
+struct TileSchedule {
+  int variant = 0;
+  int cps = 0;
+  int threads = 0;
+  float ms = 0.f;
+  float ms_default = 0.f;
+};
+int tile_block_threads(const HeomConsts &c, bool mixed, int variant);
+// Times one Liouvillian apply (L's x -> out, apply mode) for every block-size
+// variant and CTAs-per-SM cap and returns the fastest (about 30 launches).
+cudaError_t tile_autotune(const StageLaunch &L, cudaStream_t stream, TileSchedule *out);
+
 // ---- batched stages over many hierarchies (heom_tile_batch.cu) ----
 // Tiles of one hierarchy in the given arithmetic (-1 when N has no tile kernel).
 long long tile_count(const HeomConsts &c, bool mixed);

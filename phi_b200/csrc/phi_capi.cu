@@ -6,12 +6,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <complex>
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <map>
+#include <mutex>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/phi_b200.h"
@@ -21,7 +25,6 @@
 #include "heom_tile.h"
 #include "heom_timelocal.h"
 #include "heom_anneal.h"
-#include <cfloat>
 #include "phi_context.h"
 #include "phi_truncation.h"
 
@@ -274,6 +277,69 @@ void set_create_error(const std::string &msg) { g_create_error = msg; }
 
 // --------------------------------------------------------------------------
 
+namespace {
+
+// Tile-kernel schedules chosen so far in this process, per (device, N, K+1,
+// arithmetic, log2 of the node count).
+std::mutex g_sched_mu;
+std::map<std::tuple<int, int, int, int, int>, phi::TileSchedule> g_sched;
+constexpr long long kTuneMinElements = 1ll << 20;  // smaller problems keep the default schedule
+
+// The tile-shape autotuner: for a tile-eligible problem of at least
+// kTuneMinElements complex elements, times one Liouvillian apply for each
+// block-size variant and CTAs-per-SM cap (phi::tile_autotune) and keeps the
+// fastest; every result is the same bit for bit (each element's arithmetic
+// does not depend on the tile it falls in), only the time changes.
+int tune_tile_schedule(phi_ctx *ctx) {
+  if (!phi::tile_kernel_available(ctx->c)) return PHI_OK;
+  const int N = ctx->desc.num_states;
+  if (ctx->hier.M * N * N < kTuneMinElements) return PHI_OK;
+  int lg = 0;
+  for (long long m = ctx->hier.M; m > 1; m >>= 1) ++lg;
+  const auto key = std::make_tuple(ctx->desc.device, N, ctx->c.K1, ctx->mixed() ? 1 : 0, lg);
+  {
+    std::lock_guard<std::mutex> lock(g_sched_mu);
+    auto it = g_sched.find(key);
+    if (it != g_sched.end()) {
+      ctx->tile_sched = it->second;
+      ctx->c.tile_variant = it->second.variant;
+      ctx->c.tile_cps = it->second.cps;
+      return PHI_OK;
+    }
+  }
+  int rc = ctx->ensure_work(1);
+  if (rc != PHI_OK) return rc;
+  phi::StageLaunch L;
+  L.c = ctx->c;
+  L.mode = phi::kModeApply;
+  L.grid = ctx->grid;
+  L.mixed = ctx->mixed();
+  if (L.mixed) {  // complex64 input from the state, output to the other stage buffer
+    PHI_CUDA(ctx, phi::launch_to_c64(ctx->y.as<double2>(), ctx->xa.as<float2>(), ctx->hier.M, N * N,
+                                     ctx->work_stride(), ctx->stream));
+    L.xv = ctx->xa.ptr;
+    L.outv = ctx->xb.ptr;
+  } else {
+    L.xv = ctx->y.ptr;
+    L.outv = ctx->xa.ptr;
+  }
+  L.x = static_cast<const double2 *>(L.xv);
+  L.out = static_cast<double2 *>(L.outv);
+  ctx->bind_filter(L, 0);
+  phi::TileSchedule sched;
+  PHI_CUDA(ctx, phi::tile_autotune(L, ctx->stream, &sched));
+  rc = ctx->check_device_flag();
+  if (rc != PHI_OK) return rc;
+  ctx->tile_sched = sched;
+  ctx->c.tile_variant = sched.variant;
+  ctx->c.tile_cps = sched.cps;
+  std::lock_guard<std::mutex> lock(g_sched_mu);
+  g_sched[key] = sched;
+  return PHI_OK;
+}
+
+}  // namespace
+
 extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (!out) return fail(nullptr, PHI_E_INVALID, "out is NULL");
   *out = nullptr;
@@ -515,6 +581,11 @@ extern "C" int phi_gpu_create(const phi_problem_desc *desc, phi_ctx **out) {
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return fail(nullptr, PHI_E_CUDA, std::string("initial state: ") + cudaGetErrorString(e));
   ctx->time = 0.0;
+  rc = tune_tile_schedule(ctx.get());
+  if (rc != PHI_OK) {
+    g_create_error = ctx->error;
+    return rc;
+  }
   *out = ctx.release();
   return PHI_OK;
 }
@@ -721,6 +792,37 @@ extern "C" int phi_gpu_get_state(const phi_ctx *cctx, double *state) {
   if (!ctx || !state) return PHI_E_INVALID;
   PHI_CUDA(ctx, cudaMemcpyAsync(state, ctx->y.ptr, ctx->state_bytes(), cudaMemcpyDeviceToHost, ctx->stream));
   PHI_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_get_tile_schedule(const phi_ctx *ctx, phi_tile_schedule *out) {
+  if (!ctx || !out) return PHI_E_INVALID;
+  const bool tiled = phi::tile_kernel_available(ctx->c);
+  out->threads = tiled ? phi::tile_block_threads(ctx->c, ctx->mixed(), ctx->c.tile_variant) : 0;
+  out->ctas_per_sm = ctx->c.tile_cps;
+  out->ms_per_apply = ctx->tile_sched.ms;
+  out->ms_per_apply_default = ctx->tile_sched.ms_default;
+  return PHI_OK;
+}
+
+extern "C" int phi_gpu_set_tile_schedule(phi_ctx *ctx, int32_t threads, int32_t ctas_per_sm) {
+  if (!ctx) return PHI_E_INVALID;
+  if (!phi::tile_kernel_available(ctx->c)) {
+    ctx->error = "set_tile_schedule: this problem does not run on the tiled kernel";
+    return PHI_E_INVALID;
+  }
+  int variant = -1;
+  for (int v = 0; v < 2; ++v)
+    if (phi::tile_block_threads(ctx->c, ctx->mixed(), v) == threads) variant = v;
+  if (variant < 0 || ctas_per_sm < 0) {
+    ctx->error = "set_tile_schedule: threads must be " + std::to_string(phi::tile_block_threads(ctx->c, ctx->mixed(), 0)) +
+                 " or " + std::to_string(phi::tile_block_threads(ctx->c, ctx->mixed(), 1)) +
+                 " and ctas_per_sm >= 0";
+    return PHI_E_INVALID;
+  }
+  ctx->c.tile_variant = variant;
+  ctx->c.tile_cps = ctas_per_sm;
+  ctx->release_graphs();  // captured launches carry the old schedule
   return PHI_OK;
 }
 

@@ -12,6 +12,7 @@
 #include "heom_device.cuh"
 #include "heom_internal.h"
 #include "heom_kernels.h"
+#include "heom_tile.h"
 
 // Device copies of the per-term / per-element constants (HeomConsts points here).
 struct PhiConstBuffers {
@@ -105,6 +106,11 @@ struct phi_ctx {
   int ta_F = 0;
   phi::DeviceBuffer ta_hx, ta_hz, ta_V, ta_R, ta_rotate;
   std::vector<double> ta_bath0;
+
+  // Schedule of the tiled stage kernel chosen at creation (tile-eligible
+  // problems of at least kTuneMinElements elements; the choice is also in
+  // c.tile_variant / c.tile_cps).
+  phi::TileSchedule tile_sched{};
 
   double time = 0.0;
   std::string error;

@@ -370,6 +370,18 @@ class Hierarchy:
         self._restart_check(self.lib.phi_gpu_load_state(self.ctx, str(path).encode(), ctypes.byref(dt)))
         return dt.value
 
+    def tile_schedule(self) -> dict:
+        """The tiled kernel's schedule (block size, CTAs per SM cap; threads 0
+        when the problem runs on the generic kernel) and the apply times the
+        autotuner measured for it and for the default."""
+        s = capi.PhiTileSchedule()
+        self._check(self.lib.phi_gpu_get_tile_schedule(self.ctx, ctypes.byref(s)))
+        return {"threads": s.threads, "ctas_per_sm": s.ctas_per_sm, "ms_per_apply": s.ms_per_apply,
+                "ms_per_apply_default": s.ms_per_apply_default}
+
+    def set_tile_schedule(self, threads: int, ctas_per_sm: int = 0) -> None:
+        self._check(self.lib.phi_gpu_set_tile_schedule(self.ctx, int(threads), int(ctas_per_sm)))
+
     def stream_handle(self) -> int:
         s = ctypes.c_void_p()
         self._check(self.lib.phi_gpu_stream(self.ctx, ctypes.byref(s)))
