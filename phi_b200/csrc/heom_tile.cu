@@ -244,7 +244,14 @@ __global__ void __launch_bounds__(BT, TileMinBlocks<KT, MIXED, BT>::value) heom_
 #pragma unroll
     for (int b = 0; b < kMaxPre; ++b) {
       if (b >= p.npre) break;
-      if (p.pre_bytes[b] == 0) continue;  // read from global in the epilogue
+      if (p.pre_bytes[b] == 0) {
+        // Read from global memory in the epilogue (the RKF45 state y): an
+        // L2 prefetch of the tile's contiguous range now, so the epilogue's
+        // loads do not wait for DRAM.
+        if (b == 0 && p.mode == kModeRkf45)
+          bulk_prefetch_l2(p.ybuf[ycur] + (size_t)n0 * E, (uint32_t)((size_t)nt * E * sizeof(double2)));
+        continue;
+      }
       const unsigned char *src = static_cast<const unsigned char *>(p.pre[b]);
       if (b == 0 && p.mode == kModeRkf45)
         src = static_cast<const unsigned char *>(p.pre_bytes[0] == 8 ? p.y32buf[ycur] : (const void *)p.ybuf[ycur]);
