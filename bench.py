@@ -733,7 +733,7 @@ def main():
         apply_gbs = apply_bytes / (apply_ms / 1e3) / 1e9
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if os.path.exists(tpath) and WORKLOAD == "frenkel7":
+        if os.path.exists(tpath) and WORKLOAD == "frenkel7" and prec == capi.PHI_PREC_MIXED:
             try:
                 traffic = json.load(open(tpath)).get("rkf45_step_dram_bytes")
             except Exception:
