@@ -190,8 +190,13 @@ __global__ void __launch_bounds__(kSmallThreads, 1) heom_small_rk4_kernel(SmallR
     for (int s = 0; s < 4; ++s) {
       const double a = s == 2 ? dt : dt / 2;
       const double w = (s == 0 || s == 3) ? dt / 6 : dt / 3;
-      const double2 *in = s == 0 ? Y : X;
       if (RM > 0) {
+        // One item per thread: the thread combines its own two elements
+        // right away, and the stage inputs alternate between X and K (K
+        // holds X_2), so a stage needs one barrier:
+        //   stage 0: Y -> X,  1: X -> K,  2: K -> X,  3: X -> Y.
+        const double2 *in = s == 0 ? Y : (s == 2 ? K : X);
+        double2 *outb = s == 1 ? K : X;
         if (my_out0 >= 0) {
           double2 xv[RM > 0 ? RM : 1];
 #pragma unroll
@@ -204,16 +209,29 @@ __global__ void __launch_bounds__(kSmallThreads, 1) heom_small_rk4_kernel(SmallR
             v.y = fma(r_cf[r].x, xv[r].y, v.y);
             v.y = fma(r_cf[r].y, xv[r].x, v.y);
           }
-          if (my_out1 < 0) {
-            v.y = 0.0;
-            K[my_out0] = v;
-          } else {
-            K[my_out0] = v;
-            K[my_out1] = s_conj(v);
+          if (my_out1 < 0) v.y = 0.0;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int e = h == 0 ? my_out0 : my_out1;
+            if (e < 0) continue;
+            const double2 kv = h == 0 ? v : s_conj(v);
+            if (s == 0) {
+              const double2 ys = Y[e];
+              outb[e] = s_axpy(ys, kv, a);
+              ACC[e] = s_axpy(ys, kv, w);
+            } else if (s < 3) {
+              outb[e] = s_axpy(Y[e], kv, a);
+              ACC[e] = s_axpy(ACC[e], kv, w);
+            } else {
+              Y[e] = s_axpy(ACC[e], kv, w);
+            }
           }
         }
+        __syncthreads();
+        continue;
       }
-      for (long long u = RM > 0 ? items : tid; u < items; u += nth) {
+      const double2 *in = s == 0 ? Y : X;
+      for (long long u = tid; u < items; u += nth) {
         const int *ri = idx + u * R;
         const double2 *rcf = coef + u * R;
         double2 v = make_double2(0.0, 0.0);
