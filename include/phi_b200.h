@@ -149,6 +149,8 @@ typedef struct {
   int32_t converged;     /* 1 if the residual tolerance was met */
   double residual;       /* final ||r||_2 / ||b||_2 */
   double seconds;        /* device time of the solve */
+  int32_t deflated_tiers; /* tiers of the deflation space (0: plain BiCGSTAB(ell)) */
+  int32_t deflation_size; /* its dimension */
 } phi_solve_stats;
 
 /* Builds the hierarchy on the device, uploads constants and sets the initial
@@ -274,6 +276,21 @@ enum {
  * (PHI_E_NO_CONVERGENCE).  FP64 in every precision. */
 PHI_API int phi_gpu_steady_state(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t max_steps,
                                  const double *guess, phi_solve_stats *stats);
+
+/* Deflation of the steady-state solves of this context by the low tiers of
+ * the hierarchy: BiCGSTAB(ell) runs on P A y = P b with
+ * P = I - A Z (Z^T A Z)^-1 Z^T, Z the real coordinates of the ADOs of tiers
+ * 0..tiers-1 (rho_0's element (0,0) excluded), and the solution is
+ * y + Z (Z^T A Z)^-1 Z^T (b - A y): the same system, the same residual and
+ * stopping test, fewer iterations where slow population transfer sets the
+ * iteration count (PHI's own solver is undeflated: tiers = 0).  tiers = -1
+ * (the default): for ell <= 2, 2 where that space has at most 256
+ * coordinates, else 1 where rho_0's has, else 0; for ell > 2, 0; a solve
+ * deflated this way that breaks down is run again undeflated (its
+ * statistics count both runs).  tiers = 1 or 2 is refused (PHI_E_INVALID)
+ * where the space exceeds 256 coordinates.  A solve whose Galerkin matrix
+ * Z^T A Z is singular runs undeflated (stats->deflated_tiers = 0). */
+PHI_API int phi_gpu_set_steady_deflation(phi_ctx *ctx, int32_t tiers);
 
 /* Schedule of the tiled stage kernel (IndependentBath on PHI's identity site
  * map, K + 1 <= 3, N in {2..8, 10, 12, 16, 24}).  phi_gpu_create times one

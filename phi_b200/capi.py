@@ -101,6 +101,8 @@ class PhiSolveStats(ctypes.Structure):
         ("converged", c_int32),
         ("residual", c_double),
         ("seconds", c_double),
+        ("deflated_tiers", c_int32),
+        ("deflation_size", c_int32),
     ]
 
 
@@ -151,6 +153,7 @@ SIGNATURES = [
     ("phi_gpu_stream", c_int, [c_void_p, POINTER(c_void_p)]),
     ("phi_gpu_steady_state", c_int, [c_void_p, c_int32, c_double, c_int32, c_int32, c_void_p,
                                       POINTER(PhiSolveStats)]),
+    ("phi_gpu_set_steady_deflation", c_int, [c_void_p, c_int32]),
     ("phi_gpu_get_time", c_int, [c_void_p, POINTER(c_double)]),
     ("phi_gpu_set_time", c_int, [c_void_p, c_double]),
     ("phi_gpu_reset", c_int, [c_void_p, c_double]),

@@ -99,6 +99,9 @@ struct StageParams {
   // filtering (see StageLaunch)
   uint8_t *act[2];
   int act_par;
+  // apply mode, gridDim.y > 1: block row y applies to x + y * x_bstride and
+  // writes out + y * out_bstride (many inputs of one operator per launch)
+  long long x_bstride, out_bstride;
 };
 
 template <int GROUP, int KIND>
@@ -134,6 +137,10 @@ __global__ void __launch_bounds__(256) heom_stage_kernel(StageParams p) {
   const double ih = c.inv_hbar;
   double emax = 0.0;
   // RKF45 stage 0 reads the current state, whose buffer only the device knows.
+  if (gridDim.y > 1) {
+    p.x += blockIdx.y * p.x_bstride;
+    p.out += blockIdx.y * p.out_bstride;
+  }
   const double2 *xin = (p.mode == kModeRkf45 && p.stage == 0) ? p.ybuf[ycur] : p.x;
   const double2 *yin = p.mode == kModeRkf45 ? p.ybuf[ycur] : p.y;
   // Filtering: flags of the current state, and of the state this launch
@@ -558,12 +565,12 @@ __global__ void rkf45_control_kernel(Rkf45Ctl *ctl) {
 }
 
 template <int GROUP, int KIND>
-cudaError_t launch_group(const StageParams &p, size_t smem, int grid, cudaStream_t stream) {
+cudaError_t launch_group(const StageParams &p, size_t smem, int grid, int batch, cudaStream_t stream) {
   auto kern = heom_stage_kernel<GROUP, KIND>;
   static thread_local int configured[kSmemLimitDevices] = {};
   cudaError_t e = raise_smem_limit(kern, smem, configured);
   if (e != cudaSuccess) return e;
-  kern<<<grid, 256, smem, stream>>>(p);
+  kern<<<dim3(grid, batch), 256, smem, stream>>>(p);
   return cudaGetLastError();
 }
 
@@ -598,7 +605,7 @@ int stage_grid(const HeomConsts &c, int num_sms) {
 }
 
 cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream) {
-  if (tile_kernel_available(L.c)) {
+  if (!L.generic && tile_kernel_available(L.c)) {
     if (L.xv || L.outv || L.mixed) return launch_tile_stage(L, stream);
     StageLaunch T = L;  // complex128 caller: the typed pointers are the storage
     T.xv = L.x;
@@ -626,14 +633,18 @@ cudaError_t launch_stage(const StageLaunch &L, cudaStream_t stream) {
   p.act[0] = L.act[0];
   p.act[1] = L.act[1];
   p.act_par = L.act_par;
+  p.x_bstride = L.x_bstride;
+  p.out_bstride = L.out_bstride;
+  const int batch = L.batch;
+  if (batch < 1 || batch > 65535 || (batch > 1 && L.mode != kModeApply)) return cudaErrorInvalidValue;
   const size_t smem = stage_smem_bytes(L.c.N, L.c.T, L.c.kind);
   const int grid = L.grid;
   const int group = choose_group(L.c.N);
 #define PHI_DISPATCH(G)                                                      \
   switch (L.c.kind) {                                                        \
-    case kIndependent: return launch_group<G, kIndependent>(p, smem, grid, stream); \
-    case kDiagonal: return launch_group<G, kDiagonal>(p, smem, grid, stream);       \
-    default: return launch_group<G, kFull>(p, smem, grid, stream);                  \
+    case kIndependent: return launch_group<G, kIndependent>(p, smem, grid, batch, stream); \
+    case kDiagonal: return launch_group<G, kDiagonal>(p, smem, grid, batch, stream); \
+    default: return launch_group<G, kFull>(p, smem, grid, batch, stream); \
   }
   if (group == 32) {
     PHI_DISPATCH(32)

@@ -36,6 +36,13 @@ struct StageLaunch {
   // <dot_w, out> to dot_part[tile].
   const double2 *dot_w = nullptr;
   double *dot_part = nullptr;
+  // The generic kernel even where the tiled one applies (with c.M lowered,
+  // the rows of the first c.M nodes only; neighbour ids index the whole x).
+  bool generic = false;
+  // Generic kernel, apply mode: `batch` inputs at x + i * x_bstride, outputs
+  // at out + i * out_bstride (complex elements).
+  int batch = 1;
+  long long x_bstride = 0, out_bstride = 0;
   // Tiled kernel: stage input / output and k buffers in the context's
   // storage type (complex128, or complex64 in mixed precision), the
   // complex64 copies of the state, and the arithmetic.

@@ -82,7 +82,12 @@ struct phi_ctx {
   phi::DeviceBuffer bicg_parts;
   long long bicg_tiles = 0;
   int bicg_ell = 0;
+  int bicg_defl = 0;  // deflated tiers the graph was captured with
   cudaGraphExec_t bicg_graph = nullptr;
+  // Deflation of the steady-state solve (heom_deflate.cu): requested tiers
+  // (-1 automatic, 0 off) and the buffer of A Z, E^-1, g, c and the status.
+  int steady_defl = -1;
+  phi::DeviceBuffer defl_buf;
 
   // RKF45 test hooks: forced accept decisions and the per-attempt error
   // trace (phi_gpu_debug_set_rkf45_replay).

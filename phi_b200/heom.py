@@ -413,7 +413,14 @@ class Hierarchy:
         if check:
             self._check(rc)
         return {"steps": st.iterations, "converged": bool(st.converged), "residual": st.residual,
-                "seconds": st.seconds, "status": rc}
+                "seconds": st.seconds, "status": rc, "deflated_tiers": st.deflated_tiers,
+                "deflation_size": st.deflation_size}
+
+    def set_steady_deflation(self, tiers: int) -> None:
+        """Deflation of the steady-state solves by the ADOs of tiers
+        0..tiers-1: -1 automatic (the default), 0 off (PHI's plain
+        BiCGSTAB(ell)), 1 rho_0, 2 rho_0 and the first tier."""
+        self._check(self.lib.phi_gpu_set_steady_deflation(self.ctx, int(tiers)))
 
 
 class Batch:

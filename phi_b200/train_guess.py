@@ -30,10 +30,12 @@ ELL = 2
 MAX_STEPS = 40_000
 
 
-def solve(p, rho0_guess=None):
-    """One steady-state solve; returns (rho_0, stats)."""
+def solve(p, rho0_guess=None, deflation: int = 0):
+    """One steady-state solve (deflation: tiers of the deflation space, 0 =
+    PHI's plain BiCGSTAB(2)); returns (rho_0, stats)."""
     p.fix_incompatible_combinations("bicgstab")
     with Hierarchy(p) as h:
+        h.set_steady_deflation(deflation)
         st = h.steady_state(tol=TOL, ell=ELL, max_steps=MAX_STEPS, check=False, rho0_guess=rho0_guess)
         rho = h.rho0()
     return rho, st
@@ -80,8 +82,10 @@ def train(steps: int, widths=(7, 128, 128, 16), data: str = learned.DATASET, out
 
 def evaluate(count: int, weights: str = learned.WEIGHTS, seed0: int = EVAL_SEED0, log=print):
     """Plain (rho_0 = I/N start), thermal-state start and learned-guess
-    BiCGSTAB(2) on `count` held-out draws at the same tolerance.  Wall time
-    of the learned arm includes the network's inference."""
+    BiCGSTAB(2) on `count` held-out draws at the same tolerance, and the
+    solver deflated by rho_0 and the first tier (from I/N and from the
+    learned guess).  Wall time of the learned arm includes the network's
+    inference."""
     model = learned.MLP.load(weights)
     rows = []
     for k in range(count):
@@ -95,22 +99,44 @@ def evaluate(count: int, weights: str = learned.WEIGHTS, seed0: int = EVAL_SEED0
         tb = time.perf_counter() - t0
         thermal = learned.thermal_rho0(p)
         _, sc = solve(p, rho0_guess=thermal)
+        t0 = time.perf_counter()
+        rho_d, sd = solve(p, deflation=2)
+        td = time.perf_counter() - t0
+        _, sdl = solve(p, rho0_guess=guess, deflation=2)
         rows.append({"seed": seed0 + k, "plain_steps": sa["steps"], "learned_steps": sb["steps"],
                      "thermal_steps": sc["steps"],
                      "plain_device_s": sa["seconds"], "learned_device_s": sb["seconds"],
                      "plain_wall_s": ta, "learned_wall_s": tb,
                      "plain_ok": sa["status"] == capi.PHI_OK, "learned_ok": sb["status"] == capi.PHI_OK,
                      "thermal_ok": sc["status"] == capi.PHI_OK,
+                     "deflated_steps": sd["steps"], "deflated_device_s": sd["seconds"], "deflated_wall_s": td,
+                     "deflated_ok": sd["status"] == capi.PHI_OK and sd["deflated_tiers"] == 2,
+                     "deflated_learned_steps": sdl["steps"], "deflated_learned_device_s": sdl["seconds"],
+                     "deflated_learned_ok": sdl["status"] == capi.PHI_OK,
+                     "deflated_rho0_diff": float(np.abs(rho_a - rho_d).max()),
                      "rho0_diff": float(np.abs(rho_a - rho_b).max()),
                      "guess_err": float(np.abs(guess - rho_a).max()),
                      "thermal_err": float(np.abs(thermal - rho_a).max()),
                      "identity_err": float(np.abs(np.eye(p.num_states) / p.num_states - rho_a).max())})
         if k % 32 == 0:
-            log(f"eval {k}/{count}: plain {sa['steps']} learned {sb['steps']}")
+            log(f"eval {k}/{count}: plain {sa['steps']} learned {sb['steps']} deflated {sd['steps']}")
     ok = [r for r in rows if r["plain_ok"] and r["learned_ok"]]
     sum_plain = sum(r["plain_device_s"] for r in ok)
     sum_learned = sum(r["learned_device_s"] for r in ok)
+    okd = [r for r in rows if r["plain_ok"] and r["deflated_ok"] and r["deflated_learned_ok"]]
+    plain_d = sum(r["plain_device_s"] for r in okd)
     return {
+        "deflated_failed": sum(1 for r in rows if not r["deflated_ok"]),
+        "steps_deflated_mean": float(np.mean([r["deflated_steps"] for r in okd])) if okd else None,
+        "steps_deflated_learned_mean": float(np.mean([r["deflated_learned_steps"] for r in okd])) if okd else None,
+        "deflated_device_time_ratio": sum(r["deflated_device_s"] for r in okd) / plain_d if plain_d else None,
+        "deflated_learned_device_time_ratio": (sum(r["deflated_learned_device_s"] for r in okd) / plain_d
+                                               if plain_d else None),
+        "deflated_wall_time_ratio": (sum(r["deflated_wall_s"] for r in okd) / sum(r["plain_wall_s"] for r in okd)
+                                     if okd else None),
+        "max_deflated_rho0_diff": max((r["deflated_rho0_diff"] for r in okd), default=None),
+        "deflated_ms_per_solve": 1e3 * sum(r["deflated_device_s"] for r in okd) / len(okd) if okd else None,
+        "plain_ms_per_solve": 1e3 * plain_d / len(okd) if okd else None,
         "draws": count, "both_converged": len(ok),
         "plain_failed": sum(1 for r in rows if not r["plain_ok"]),
         "learned_failed": sum(1 for r in rows if not r["learned_ok"]),
