@@ -185,6 +185,53 @@ __device__ bool cta_invert(double *A, int n, int *swaps, double *prow, double *p
   return true;
 }
 
+// In-place inverse of the n x n row-major matrix A (n <= 32, shared
+// memory) by one warp, the same elimination as cta_invert: lane c owns
+// column c during the elimination and row c during the column exchanges.
+// Returns false in every lane if a pivot is zero or not finite.
+__device__ bool warp_invert(double *A, int n, int *swaps) {
+  const int lane = threadIdx.x & 31;
+  for (int p = 0; p < n; ++p) {
+    double best = lane >= p && lane < n ? fabs(A[lane * n + p]) : -1.0;
+    int bi = lane >= p && lane < n ? lane : n;
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) {
+        best = ov;
+        bi = oi;
+      }
+    }
+    if (!(best > 0.0) || !(best - best == 0.0) || bi >= n) return false;  // uniform: every lane holds the result
+    if (lane == 0) swaps[p] = bi;
+    if (lane < n && bi != p) {
+      const double t = A[p * n + lane];
+      A[p * n + lane] = A[bi * n + lane];
+      A[bi * n + lane] = t;
+    }
+    __syncwarp();
+    const double inv = 1.0 / A[p * n + p];
+    const double prow = lane < n ? (lane == p ? 1.0 : A[p * n + lane]) * inv : 0.0;
+    const double pcol = lane < n ? A[lane * n + p] : 0.0;
+    __syncwarp();
+    for (int i = 0; i < n; ++i) {
+      const double f = __shfl_sync(0xffffffffu, pcol, i);
+      if (lane < n) A[i * n + lane] = i == p ? prow : (lane == p ? 0.0 : A[i * n + lane]) - f * prow;
+    }
+    __syncwarp();
+  }
+  for (int p = n - 1; p >= 0; --p) {
+    const int r = swaps[p];
+    if (lane < n && r != p) {
+      const double t = A[lane * n + p];
+      A[lane * n + p] = A[lane * n + r];
+      A[lane * n + r] = t;
+    }
+    __syncwarp();
+  }
+  return true;
+}
+
 // Factors E = Z^T A Z: A01, the inverses of the first-tier blocks of D,
 // F = D^-1 A10 and the inverse of S = A00 - A01 F.  One CTA; matrices of at
 // most kSmemDoubles entries are inverted in shared memory (mat_s).
@@ -198,17 +245,42 @@ __global__ void __launch_bounds__(kSolveBlock) factor_kernel(DeflView D) {
     const int p = idx / n1, i = idx - p * n1;
     D.A01[idx] = galerkin(D, p, k0 + i);
   }
-  double *Mb = E * E <= kSmemDoubles ? mat_s : D.work;
-  for (int a = 0; a < t1; ++a) {
-    const int o = k0 + a * E;
-    for (int idx = tid; idx < E * E; idx += nt) Mb[idx] = galerkin(D, o + idx / E, o + idx % E);
+  const int regions = t1 < nw ? t1 : nw;
+  if (E <= 32 && regions * E * E <= kSmemDoubles) {
+    // one warp per block, each in its own region of shared memory
+    __shared__ int wswaps[kSolveBlock / 32][32];
+    if (tid == 0) bad = 0;
     __syncthreads();
-    if (!cta_invert(Mb, E, swaps, prow, pcol, wv, wi, &bad)) {
+    double *Mw = mat_s + warp * E * E;
+    for (int a = warp; a < t1; a += nw) {
+      const int o = k0 + a * E;
+      for (int idx = lane; idx < E * E; idx += 32) Mw[idx] = galerkin(D, o + idx / E, o + idx % E);
+      __syncwarp();
+      if (!warp_invert(Mw, E, wswaps[warp])) {
+        if (lane == 0) bad = 1;
+        break;
+      }
+      for (int idx = lane; idx < E * E; idx += 32) D.Dinv[(long long)a * E * E + idx] = Mw[idx];
+      __syncwarp();
+    }
+    __syncthreads();
+    if (bad) {
       if (tid == 0) *D.status = 1;
       return;
     }
-    for (int idx = tid; idx < E * E; idx += nt) D.Dinv[(long long)a * E * E + idx] = Mb[idx];
-    __syncthreads();
+  } else {
+    double *Mb = E * E <= kSmemDoubles ? mat_s : D.work;
+    for (int a = 0; a < t1; ++a) {
+      const int o = k0 + a * E;
+      for (int idx = tid; idx < E * E; idx += nt) Mb[idx] = galerkin(D, o + idx / E, o + idx % E);
+      __syncthreads();
+      if (!cta_invert(Mb, E, swaps, prow, pcol, wv, wi, &bad)) {
+        if (tid == 0) *D.status = 1;
+        return;
+      }
+      for (int idx = tid; idx < E * E; idx += nt) D.Dinv[(long long)a * E * E + idx] = Mb[idx];
+      __syncthreads();
+    }
   }
   for (int idx = tid; idx < n1 * k0; idx += nt) {
     const int i = idx / k0, q = idx - i * k0;
@@ -263,6 +335,7 @@ __global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const do
     const double *drow = D.Dinv + (long long)i * E;
     const double *zb = z + k0 + (i / E) * E;
     double s = 0.0;
+#pragma unroll 8
     for (int t = 0; t < E; ++t) s = fma(drow[t], zb[t], s);
     w[i] = s;
   }
@@ -284,6 +357,7 @@ __global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const do
   for (int i = tid; i < n1; i += nt) {
     const double *frow = D.F + (long long)i * k0;
     double s = 0.0;
+#pragma unroll 8
     for (int q = 0; q < k0; ++q) s = fma(frow[q], cs[q], s);
     cs[k0 + i] = w[i] - s;
   }
@@ -357,7 +431,10 @@ cudaError_t defl_launch_factor(const DeflView &D, cudaStream_t st) {
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   const int big = D.E > D.k0 ? D.E : D.k0;
-  const long long need = (long long)big * big;
+  const int t1 = D.n1 / D.E, regions = t1 < kSolveBlock / 32 ? t1 : kSolveBlock / 32;
+  long long need = (long long)big * big;
+  if (D.E <= 32 && (long long)regions * D.E * D.E <= kSmemDoubles && (long long)regions * D.E * D.E > need)
+    need = (long long)regions * D.E * D.E;  // one region per warp for the first-tier blocks
   const size_t smem = (size_t)(need < kSmemDoubles ? need : kSmemDoubles) * sizeof(double);
   e = cudaFuncSetAttribute(factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

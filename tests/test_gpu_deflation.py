@@ -20,6 +20,8 @@ PROBLEMS = [
     ("indep_n3_K2_L4", lambda: cases.random_problem("independent", n=3, matsubara=2, truncation=4, seed=3)),
     ("diag_n3_b2_K1_L4", lambda: cases.random_problem("diagonal", n=3, matsubara=1, truncation=4, baths=2, seed=3)),
     ("full_n2_b2_K2_L4", lambda: cases.random_problem("full", n=2, matsubara=2, truncation=4, baths=2, seed=3)),
+    # 36 coordinates per ADO: first-tier blocks inverted by the whole CTA instead of one warp each
+    ("indep_n6_K1_L3", lambda: cases.random_problem("independent", n=6, matsubara=1, truncation=3, seed=4)),
 ]
 
 
