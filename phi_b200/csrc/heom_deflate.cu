@@ -43,6 +43,8 @@ constexpr int kSolveBlock = 1024;
 // Matrices of the factorisation up to this many doubles are inverted in
 // shared memory, larger ones in the global work buffer (L2).
 constexpr int kSmemDoubles = 16384;
+// The projection's factors are staged in shared memory up to this size.
+constexpr int kStageDoubles = 24576;
 
 __device__ __forceinline__ double cdot_re(double2 a, double2 b) { return a.x * b.x + a.y * b.y; }
 
@@ -321,11 +323,23 @@ __global__ void g_kernel(DeflView D, const double2 *rhat) {
 
 // c = E^-1 Z^T (v - b) through the factors: w = D^-1 z1,
 // c0 = S^-1 (z0 - A01 w), c1 = w - F c0; *part = -<g, c>.  One CTA.
+// The factors (Dinv, F, A01, Si: one contiguous run of doubles) are first
+// copied into shared memory when they fit (stage = true).
 __global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const double2 *v, const double2 *b,
-                                                          double *part) {
+                                                          double *part, bool stage) {
+  extern __shared__ double fac_s[];
   __shared__ double z[kMaxDeflK], w[kMaxDeflK], cs[kMaxDeflK];
+  if (D.done && *(volatile const int *)D.done) return;  // uniform: the solve has stopped
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int E = D.E, k0 = D.k0, n1 = D.n1, k = D.k;
+  if (stage) {
+    const long long total = (long long)n1 * E + 2ll * n1 * k0 + (long long)k0 * k0;
+    for (long long i = tid; i < total; i += nt) fac_s[i] = D.Dinv[i];
+    D.Dinv = fac_s;
+    D.F = D.Dinv + (long long)n1 * E;
+    D.A01 = D.F + (long long)n1 * k0;
+    D.Si = D.A01 + (long long)k0 * n1;
+  }
   for (int p = tid; p < k; p += nt) {
     const Coord c = coord_of(p + 1, D.N);
     z[p] = zcoord(v, c, D.N) - (b ? zcoord(b, c, D.N) : 0.0);
@@ -375,6 +389,7 @@ __global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const do
 // row of the row-major copy, lanes over j.
 __global__ void update_kernel(DeflView D, double2 *v) {
   __shared__ double cs[kMaxDeflK];
+  if (D.done && *(volatile const int *)D.done) return;
   for (int j = threadIdx.x; j < D.k; j += blockDim.x) cs[j] = D.c[j];
   __syncthreads();
   const int lane = threadIdx.x & 31;
@@ -449,7 +464,15 @@ cudaError_t defl_launch_g(const DeflView &D, const double2 *rhat, cudaStream_t s
 }
 
 cudaError_t defl_launch_coeff(const DeflView &D, const double2 *v, const double2 *b, double *part, cudaStream_t st) {
-  coeff_kernel<<<1, kSolveBlock, 0, st>>>(D, v, b, part);
+  const long long total = (long long)D.n1 * D.E + 2ll * D.n1 * D.k0 + (long long)D.k0 * D.k0;
+  const bool stage = total <= kStageDoubles;
+  const size_t smem = stage ? (size_t)total * sizeof(double) : 0;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(coeff_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kStageDoubles * sizeof(double)));
+    if (e != cudaSuccess) return e;
+  }
+  coeff_kernel<<<1, kSolveBlock, smem, st>>>(D, v, b, part, stage);
   return cudaGetLastError();
 }
 

@@ -31,6 +31,7 @@ struct DeflView {
   double *c;         // k: coefficients of the last projection
   double *work;      // scratch of the factorisation: max(k0, E)^2
   int *status;       // 0 ok, 1 the Galerkin matrix is singular
+  const int *done;   // the solver's stop flag: projections return at once once it is set (NULL: always run)
   double2 *units;    // k unit inputs of unit_len elements (setup only)
 };
 

@@ -305,6 +305,10 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     if (status == 0) defl_tiers = plan.tiers;
   }
   const phi::DeflView *Dp = defl_tiers > 0 ? &D : nullptr;
+  // The projections inside the iteration stop with the solver; the initial
+  // and final ones (D itself, done == NULL) always run.
+  phi::DeflView Dloop = D;
+  Dloop.done = &sc->done;
   // b = -L(E00), element (0,0) of node 0 dropped.
   const double2 one = make_double2(1.0, 0.0);
   PHI_SK(cudaMemsetAsync(V.r[0], 0, bytes, s));
@@ -351,7 +355,7 @@ int steady_impl(phi_ctx *ctx, int32_t ell, double tol, int32_t tol_mode, int32_t
     PHI_SK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     cudaError_t eb = cudaSuccess;
     for (int it = 0; it < outer_per_graph && eb == cudaSuccess; ++it)
-      eb = outer_iteration(ctx, V, n, sc, ell, grid, s, Dp);
+      eb = outer_iteration(ctx, V, n, sc, ell, grid, s, Dp ? &Dloop : nullptr);
     cudaError_t ee = cudaStreamEndCapture(s, &graph);
     if (eb != cudaSuccess || ee != cudaSuccess) {
       if (graph) cudaGraphDestroy(graph);
