@@ -37,9 +37,11 @@ struct DeflView {
 
 // The unit inputs: units + j * unit_len holds Z_j (zeros elsewhere).
 cudaError_t defl_launch_units(const DeflView &D, cudaStream_t st);
-// After the batched apply wrote A Z: zero element (0,0) of node 0 of every
-// column (that equation is dropped), copy A Z row-major, and factor the
-// Galerkin matrix (one CTA; status 1 if a pivot is zero or not finite).
+// After the batched apply wrote A Z: copy it row-major with element (0,0)
+// of node 0 zeroed in every column (that equation is dropped; the
+// column-major copy is only read at deflated coordinates, which exclude
+// it), and factor the Galerkin matrix (one CTA; status 1 if a pivot is zero
+// or not finite).
 cudaError_t defl_launch_factor(const DeflView &D, cudaStream_t st);
 // g_j = <rhat, A Z_j>.
 cudaError_t defl_launch_g(const DeflView &D, const double2 *rhat, cudaStream_t st);
