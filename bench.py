@@ -53,8 +53,9 @@ def parse_args():
     ap.add_argument("--workload", default="frenkel7",
                     choices=["frenkel7", "ring24", "batched", "steady", "spin_boson"],
                     help="frenkel7: the RKF45 headline (7-site exciton); ring24: 24-site ring RKF45; "
-                         "batched: 512 uneven RK4 instances; steady: chain4 steady states, plain vs "
-                         "learned initial guess; spin_boson: the 11-node RK4 configuration")
+                         "batched: 512 uneven RK4 instances; steady: chain4 steady states, undeflated and "
+                         "deflated, from I/N and from the learned initial guess; spin_boson: the 11-node "
+                         "RK4 configuration")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--draws", type=int, default=32, help="steady workload: held-out draws")
     return ap.parse_args()
