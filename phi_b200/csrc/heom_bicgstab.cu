@@ -207,7 +207,6 @@ __global__ void gamma_kernel(BicgVectors V, long long n, BicgScalars *sc, int j)
   }
 }
 
-// r_i -= alpha u_{i+1} for i = 0..j; x += alpha u_0.
 // rho_kernel / gamma_kernel's scalar steps from per-tile partial sums of
 // <rhat, .> (the apply zeroed element 0 and summed them); one block, summed
 // in tile order (deterministic).
@@ -217,23 +216,10 @@ __global__ void dot_finish_kernel(const double *parts, long long nparts, BicgSca
   for (long long b = threadIdx.x; b < nparts; b += kBlock) v[0] += parts[b];
   block_sum<1>(v);
   if (threadIdx.x != 0) return;
-  const double tot = v[0];
-  if (which == 0) {
-    if (!finite(tot)) {
-      fail(sc, kBicgNonFinite);
-    } else if (sc->rho0 == 0.0 || tot == 0.0) {
-      fail(sc, kBicgRhoZero);
-    } else {
-      sc->beta = sc->alpha * tot / sc->rho0;
-      sc->rho0 = tot;
-    }
-  } else {
-    if (!finite(tot)) fail(sc, kBicgNonFinite);
-    else if (tot == 0.0) fail(sc, kBicgGammaZero);
-    else sc->alpha = sc->rho0 / tot;
-  }
+  bicg_dot_step(sc, v[0], which);
 }
 
+// r_i -= alpha u_{i+1} for i = 0..j; x += alpha u_0.
 __global__ void r_update_kernel(BicgVectors V, long long n, const BicgScalars *sc, int j) {
   if (solve_done(sc)) return;
   const double a = sc->alpha;

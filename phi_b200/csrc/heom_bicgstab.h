@@ -38,6 +38,34 @@ struct BicgScalars {
   double partials[kMaxGramDots * kMaxBicgBlocks];
 };
 
+#ifdef __CUDACC__
+// The scalar step once <rhat, .> is summed (one thread): which = 0, rho --
+// beta = alpha rho_new / rho_old and the new rho, a breakdown if either
+// vanishes; which = 1, gamma -- alpha = rho / gamma.  A non-finite sum stops
+// the solve.
+__device__ inline void bicg_dot_step(BicgScalars *sc, double tot, int which) {
+  int code = kBicgOk;
+  if (!(tot == tot && tot - tot == 0.0)) {
+    code = kBicgNonFinite;
+  } else if (which == 0) {
+    if (sc->rho0 == 0.0 || tot == 0.0) {
+      code = kBicgRhoZero;
+    } else {
+      sc->beta = sc->alpha * tot / sc->rho0;
+      sc->rho0 = tot;
+    }
+  } else if (tot == 0.0) {
+    code = kBicgGammaZero;
+  } else {
+    sc->alpha = sc->rho0 / tot;
+  }
+  if (code != kBicgOk) {
+    sc->breakdown = code;
+    sc->done = 1;
+  }
+}
+#endif
+
 int bicg_grid(int num_sms);
 // b = -b with element (0,0) of node 0 zeroed (b holds L(E00) on entry).
 cudaError_t bicg_launch_rhs(double2 *b, long long n, int grid, cudaStream_t s);

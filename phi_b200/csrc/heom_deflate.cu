@@ -33,6 +33,7 @@
 // (Z_q = i E_ji - i E_ij).
 #include <cuda_runtime.h>
 
+#include "heom_bicgstab.h"
 #include "heom_deflate.h"
 
 namespace phi {
@@ -325,11 +326,9 @@ __global__ void g_kernel(DeflView D, const double2 *rhat) {
 // c0 = S^-1 (z0 - A01 w), c1 = w - F c0; *part = -<g, c>.  One CTA.
 // The factors (Dinv, F, A01, Si: one contiguous run of doubles) are first
 // copied into shared memory when they fit (stage = true).
-__global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const double2 *v, const double2 *b,
-                                                          double *part, bool stage) {
-  extern __shared__ double fac_s[];
+__device__ __forceinline__ void coeff_body(DeflView D, const double2 *v, const double2 *b, double *part,
+                                           bool stage, double *fac_s) {
   __shared__ double z[kMaxDeflK], w[kMaxDeflK], cs[kMaxDeflK];
-  if (D.done && *(volatile const int *)D.done) return;  // uniform: the solve has stopped
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
   const int E = D.E, k0 = D.k0, n1 = D.n1, k = D.k;
   if (stage) {
@@ -382,6 +381,38 @@ __global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const do
     for (int j = lane; j < k; j += 32) s = fma(D.g[j], cs[j], s);
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if (lane == 0) *part = -s;
+  }
+}
+
+__global__ void __launch_bounds__(kSolveBlock) coeff_kernel(DeflView D, const double2 *v, const double2 *b,
+                                                          double *part, bool stage) {
+  extern __shared__ double fac_s[];
+  if (D.done && *(volatile const int *)D.done) return;  // uniform: the solve has stopped
+  coeff_body(D, v, b, part, stage, fac_s);
+}
+
+// The coefficients of v's projection, then the BiCG scalar step of the
+// inner product whose per-tile partials the apply left in parts[0..nparts-1]
+// (the projection's change is parts[nparts-1] = *part): one launch instead
+// of a coefficient kernel and a one-block finish.  Summed in part order.
+__global__ void __launch_bounds__(kSolveBlock) coeff_finish_kernel(DeflView D, const double2 *v, double *part,
+                                                                 const double *parts, long long nparts,
+                                                                 BicgScalars *sc, int which, bool stage) {
+  extern __shared__ double fac_s[];
+  __shared__ double red[kSolveBlock / 32];
+  if (D.done && *(volatile const int *)D.done) return;  // uniform: the solve has stopped
+  coeff_body(D, v, nullptr, part, stage, fac_s);
+  __syncthreads();  // *part is visible to the whole CTA
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s = 0.0;
+  for (long long i = threadIdx.x; i < nparts; i += blockDim.x) s += parts[i];
+  for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+  if (lane == 0) red[warp] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red[i];
+    bicg_dot_step(sc, tot, which);
   }
 }
 
@@ -473,6 +504,20 @@ cudaError_t defl_launch_coeff(const DeflView &D, const double2 *v, const double2
     if (e != cudaSuccess) return e;
   }
   coeff_kernel<<<1, kSolveBlock, smem, st>>>(D, v, b, part, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t defl_launch_coeff_finish(const DeflView &D, const double2 *v, double *part, const double *parts,
+                                     long long nparts, BicgScalars *sc, int which, cudaStream_t st) {
+  const long long total = (long long)D.n1 * D.E + 2ll * D.n1 * D.k0 + (long long)D.k0 * D.k0;
+  const bool stage = total <= kStageDoubles;
+  const size_t smem = stage ? (size_t)total * sizeof(double) : 0;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(coeff_finish_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kStageDoubles * sizeof(double)));
+    if (e != cudaSuccess) return e;
+  }
+  coeff_finish_kernel<<<1, kSolveBlock, smem, st>>>(D, v, part, parts, nparts, sc, which, stage);
   return cudaGetLastError();
 }
 

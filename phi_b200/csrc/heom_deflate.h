@@ -6,6 +6,8 @@
 
 namespace phi {
 
+struct BicgScalars;
+
 // Largest deflation space: the coordinates of the deflated tiers' ADOs.
 constexpr int kMaxDeflK = 256;
 
@@ -48,6 +50,11 @@ cudaError_t defl_launch_g(const DeflView &D, const double2 *rhat, cudaStream_t s
 // c = (Z^T A Z)^-1 Z^T (v - b) (b may be NULL); with part != NULL also
 // *part = -<g, c>, the change of <rhat, v> made by the update below.
 cudaError_t defl_launch_coeff(const DeflView &D, const double2 *v, const double2 *b, double *part, cudaStream_t st);
+// defl_launch_coeff (without b, part != NULL) followed by the BiCG scalar
+// step of the inner product summed from parts[0..nparts-1], whose last
+// entry is *part (rho: which = 0, gamma: which = 1), in one launch.
+cudaError_t defl_launch_coeff_finish(const DeflView &D, const double2 *v, double *part, const double *parts,
+                                     long long nparts, BicgScalars *sc, int which, cudaStream_t st);
 // v -= A Z c over the rows of tiers 0..tiers: v becomes P v with
 // P = I - A Z (Z^T A Z)^-1 Z^T (after defl_launch_coeff without b), or
 // b - v becomes P (b - v) (with b).

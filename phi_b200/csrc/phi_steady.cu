@@ -70,19 +70,31 @@ cudaError_t outer_iteration(phi_ctx *ctx, const phi::BicgVectors &V, long long n
   const long long nparts = tiles + (D ? 1 : 0);
   double *pu = fused ? ctx->bicg_parts.as<double>() : nullptr;
   double *pr = fused ? pu + tiles + 1 : nullptr;
+  // Deflated and fused, the projection's coefficient kernel also finishes
+  // the inner product (rho or gamma) before its update kernel runs.
+  const bool fold = fused && D;
   for (int j = 0; j < ell && e == cudaSuccess; ++j) {
-    if (j > 0) e = fused ? phi::bicg_launch_dot_finish(pr, nparts, sc, 0, s)
-                         : phi::bicg_launch_rho(V, n, sc, j, grid, s);
+    if (j > 0 && !fold)
+      e = fused ? phi::bicg_launch_dot_finish(pr, nparts, sc, 0, s) : phi::bicg_launch_rho(V, n, sc, j, grid, s);
     if (e == cudaSuccess) e = phi::bicg_launch_u_update(V, n, sc, j, grid, s);
     if (e == cudaSuccess) e = apply_fp64(ctx, V.u[j], V.u[j + 1], s, fused ? V.rhat : nullptr, pu);
-    if (e == cudaSuccess && D) e = project(D, V.u[j + 1], fused ? pu + tiles : nullptr, s);
-    if (e == cudaSuccess)
-      e = fused ? phi::bicg_launch_dot_finish(pu, nparts, sc, 1, s)
-                : phi::bicg_launch_gamma(V, n, sc, j, grid, s);
+    if (e == cudaSuccess && fold) {
+      e = phi::defl_launch_coeff_finish(*D, V.u[j + 1], pu + tiles, pu, nparts, sc, 1, s);
+      if (e == cudaSuccess) e = phi::defl_launch_update(*D, V.u[j + 1], s);
+    } else {
+      if (e == cudaSuccess && D) e = project(D, V.u[j + 1], nullptr, s);
+      if (e == cudaSuccess)
+        e = fused ? phi::bicg_launch_dot_finish(pu, nparts, sc, 1, s) : phi::bicg_launch_gamma(V, n, sc, j, grid, s);
+    }
     if (e == cudaSuccess) e = phi::bicg_launch_r_update(V, n, sc, j, grid, s);
     const bool rho_next = fused && j + 1 < ell;  // the last r_{j+1} goes to the Gram step instead
     if (e == cudaSuccess) e = apply_fp64(ctx, V.r[j], V.r[j + 1], s, rho_next ? V.rhat : nullptr, pr);
-    if (e == cudaSuccess && D) e = project(D, V.r[j + 1], rho_next ? pr + tiles : nullptr, s);
+    if (e == cudaSuccess && fold && rho_next) {
+      e = phi::defl_launch_coeff_finish(*D, V.r[j + 1], pr + tiles, pr, nparts, sc, 0, s);
+      if (e == cudaSuccess) e = phi::defl_launch_update(*D, V.r[j + 1], s);
+    } else if (e == cudaSuccess && D) {
+      e = project(D, V.r[j + 1], nullptr, s);
+    }
   }
   if (e == cudaSuccess) e = phi::bicg_launch_gram(V, n, sc, ell, grid, s);
   if (e == cudaSuccess) e = phi::bicg_launch_mr_update(V, n, sc, ell, grid, s);
